@@ -1,0 +1,260 @@
+// Fixture harness around the reference's own public C++ API (test
+// infrastructure; never linked into the CUDA product).
+//
+// Each entry point calls the reference's classes exactly as its driver does
+// (include/euler.hpp:161-249): Problem construction (problem.cpp:32), Initial
+// (problem.cpp:329), Freeze (350), Residual (445), PartialDG Mult / Diagonal
+// blocks (partial.cpp:62, 265), PrepareHybrid + StreamCondense
+// (condensation.cpp:47, 131), the condensed Schur operator Mult
+// (operators.cpp:147), its Jacobi panels (operators.cpp:275), Recover
+// (condensation.cpp:154) and LinearSolver::Solve (linear.cpp:167). Compiled
+// against the MFEM-subset shim into oracle/_ref/libeuler_ref.so.
+#include "euler.hpp"
+
+#include <cstring>
+#include <memory>
+
+using namespace euler;
+
+namespace {
+struct RefHandle {
+  Options opt;
+  std::unique_ptr<EulerGas> gas;
+  std::unique_ptr<Problem> p;
+  Hybrid h;
+  Condensed s;
+  bool hybrid_ready = false;
+  std::string err;
+};
+thread_local std::string g_err;
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+}  // namespace
+
+extern "C" {
+const char *ref_last_error() { return g_err.c_str(); }
+
+// assembly: 0 partial, 1 full; precond: 0 block-jacobi, 1 block-ilu0.
+void *ref_problem_new(int nx, int ny, int k, double alpha_deg, double safety, int assembly,
+                      int precond, int restart, int max_krylov, double linear_tol) {
+  auto *hd = new RefHandle();
+  int rc = guarded([&] {
+    hd->opt.nx = nx;
+    hd->opt.ny = ny;
+    hd->opt.k = k;
+    hd->opt.alpha = alpha_deg;
+    hd->opt.safety = safety;
+    hd->opt.assembly = assembly ? "full" : "partial";
+    hd->opt.matrix_free = assembly == 0;
+    hd->opt.precond = precond ? "block-ilu0" : "block-jacobi";
+    hd->opt.restart = restart;
+    hd->opt.max_krylov = max_krylov;
+    hd->opt.linear_tol = linear_tol;
+    hd->opt.steps = 1;
+    hd->gas = std::make_unique<EulerGas>(3.);
+    hd->p = std::make_unique<Problem>(hd->opt, *hd->gas);
+  });
+  if (rc) {
+    delete hd;
+    return nullptr;
+  }
+  return hd;
+}
+void ref_problem_free(void *h) { delete static_cast<RefHandle *>(h); }
+
+// out: n, p, m, t, nf, nu, nl
+void ref_sizes(void *hv, int *out) {
+  auto &p = *static_cast<RefHandle *>(hv)->p;
+  const int v[7] = {p.n, p.p, p.m, p.t, p.nf, p.nu, p.nl};
+  std::memcpy(out, v, sizeof v);
+}
+// geometry: lx, ly, hx, hy, area
+void ref_geometry(void *hv, double *out) {
+  auto &p = *static_cast<RefHandle *>(hv)->p;
+  const double v[5] = {p.lx, p.ly, p.hx, p.hy, p.area};
+  std::memcpy(out, v, sizeof v);
+}
+// Tables: w[p], ew[q], inv_mass_diag[p], mass_diag[p], tensor_dx[q*q] (a,i row-major
+// a*q+i), tensor_dy[q*q], fv[4][q][p] (side, face point, node), tensor_node[p].
+void ref_tables(void *hv, double *w, double *ew, double *inv_mass, double *mass, double *tdx,
+                double *tdy, double *fv, int *tensor_node) {
+  auto &p = *static_cast<RefHandle *>(hv)->p;
+  const int q = p.opt.k + 1;
+  for (int i = 0; i < p.p; ++i) {
+    w[i] = p.w[i];
+    inv_mass[i] = p.inv_mass(i, i);
+    mass[i] = p.mass(i, i);
+    tensor_node[i] = p.tensor_node[i];
+  }
+  for (int i = 0; i < q; ++i) ew[i] = p.ew[i];
+  for (int a = 0; a < q; ++a)
+    for (int i = 0; i < q; ++i) {
+      tdx[a * q + i] = p.tensor_dx(a, i);
+      tdy[a * q + i] = p.tensor_dy(a, i);
+    }
+  for (int s = 0; s < 4; ++s)
+    for (int qq = 0; qq < q; ++qq)
+      for (int i = 0; i < p.p; ++i) fv[(s * q + qq) * p.p + i] = p.fv[s](qq, i);
+}
+int ref_initial(void *hv, double *u) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    Vector v = p.Initial();
+    std::memcpy(u, v.GetData(), sizeof(double) * p.nu);
+  });
+}
+// Freeze at state u with stage step dt; outputs per face point a, b (nf*q each)
+// and the CFL wave rate.
+int ref_freeze(void *hv, const double *u, double dt, int check_admissible, double *a, double *b,
+               double *rate) {
+  return guarded([&] {
+    auto *hd = static_cast<RefHandle *>(hv);
+    auto &p = *hd->p;
+    Vector uv(const_cast<double *>(u), p.nu);
+    p.Freeze(uv, dt, check_admissible != 0);
+    const int q = p.opt.k + 1;
+    for (int f = 0; f < p.nf; ++f)
+      for (int j = 0; j < q; ++j) {
+        a[f * q + j] = p.faces[f].a[j];
+        b[f * q + j] = p.faces[f].b[j];
+      }
+    *rate = p.WaveRate();
+    hd->hybrid_ready = false;
+  });
+}
+int ref_set_old(void *hv, const double *old) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    std::memcpy(p.old.GetData(), old, sizeof(double) * p.nu);
+  });
+}
+void ref_set_dt(void *hv, double dt) { static_cast<RefHandle *>(hv)->p->dt = dt; }
+int ref_residual(void *hv, const double *u, double *r) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    Vector uv(const_cast<double *>(u), p.nu), rv(r, p.nu);
+    p.Residual(uv, rv);
+  });
+}
+double ref_cell_norm(void *hv, const double *r) {
+  auto &p = *static_cast<RefHandle *>(hv)->p;
+  Vector rv(const_cast<double *>(r), p.nu);
+  return p.CellNorm(rv);
+}
+int ref_admissible(void *hv, const double *u) {
+  auto &p = *static_cast<RefHandle *>(hv)->p;
+  Vector uv(const_cast<double *>(u), p.nu);
+  return p.Admissible(uv) ? 1 : 0;
+}
+// y = J(u) x with the partially assembled DG Jacobian.
+int ref_dg_apply(void *hv, const double *u, const double *x, double *y) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    Vector uv(const_cast<double *>(u), p.nu), xv(const_cast<double *>(x), p.nu), yv(y, p.nu);
+    auto op = p.PartialDG(uv);
+    op->Mult(xv, yv);
+  });
+}
+// Unfactored DG block-Jacobi diagonal blocks, n blocks of m*m column-major.
+int ref_dg_jacobi_blocks(void *hv, const double *u, double *blocks) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    Vector uv(const_cast<double *>(u), p.nu);
+    auto op = p.PartialDG(uv);
+    std::vector<DenseMatrix> d;
+    op->DiagonalBlocks(p.m, d);
+    for (int e = 0; e < p.n; ++e)
+      std::memcpy(blocks + size_t(e) * p.m * p.m, d[e].GetData(), sizeof(double) * p.m * p.m);
+  });
+}
+// Streamed HDG condensation at state u with residual r. Outputs rhs (nl),
+// X (n blocks of m x 4t column-major), y (nu), D (nl).
+int ref_hdg_condense(void *hv, const double *u, const double *r, double *rhs, double *X, double *y,
+                     double *D) {
+  return guarded([&] {
+    auto *hd = static_cast<RefHandle *>(hv);
+    auto &p = *hd->p;
+    if (!hd->hybrid_ready) {
+      hd->h = Hybrid();
+      hd->s = Condensed();
+      p.PrepareHybrid(hd->h, hd->s);
+      hd->hybrid_ready = true;
+    }
+    Vector uv(const_cast<double *>(u), p.nu), rv(const_cast<double *>(r), p.nu);
+    p.StreamCondense(uv, rv, hd->h, hd->s);
+    std::memcpy(rhs, hd->s.rhs.GetData(), sizeof(double) * p.nl);
+    std::memcpy(D, hd->h.D.GetData(), sizeof(double) * p.nl);
+    const int xs = p.m * 4 * p.t;
+    for (int e = 0; e < p.n; ++e) {
+      std::memcpy(X + size_t(e) * xs, hd->s.X[e].GetData(), sizeof(double) * xs);
+      std::memcpy(y + size_t(e) * p.m, hd->s.y[e].GetData(), sizeof(double) * p.m);
+    }
+  });
+}
+int ref_schur_apply(void *hv, const double *v, double *sv) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    auto &s = static_cast<RefHandle *>(hv)->s;
+    Vector vv(const_cast<double *>(v), p.nl), out(sv, p.nl);
+    s.op->Mult(vv, out);
+  });
+}
+// Schur block-Jacobi diagonal blocks (nf blocks of t*t column-major), unfactored.
+int ref_schur_jacobi_blocks(void *hv, double *blocks) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    auto &s = static_cast<RefHandle *>(hv)->s;
+    std::vector<DenseMatrix> d;
+    s.op->DiagonalBlocks(p.t, d);
+    for (int f = 0; f < p.nf; ++f)
+      std::memcpy(blocks + size_t(f) * p.t * p.t, d[f].GetData(), sizeof(double) * p.t * p.t);
+  });
+}
+int ref_recover(void *hv, const double *lam, double *du) {
+  return guarded([&] {
+    auto &p = *static_cast<RefHandle *>(hv)->p;
+    auto &s = static_cast<RefHandle *>(hv)->s;
+    Vector lv(const_cast<double *>(lam), p.nl), dv(du, p.nu);
+    p.Recover(s, lv, dv);
+  });
+}
+// One linear solve with the persistent weighted GMRES (linear.cpp:167).
+// form 0: DG Jacobian J(u) x = rhs (nu); form 1: condensed Schur S x = rhs (nl)
+// using the last ref_hdg_condense. Outputs x, the equation residual
+// (J x - rhs), the Krylov count and the relative residual.
+int ref_linear_solve(void *hv, int form, const double *u, const double *rhs, double *x,
+                     double *eq_residual, int *count, double *relres) {
+  return guarded([&] {
+    auto *hd = static_cast<RefHandle *>(hv);
+    auto &p = *hd->p;
+    const int nsz = form == 0 ? p.nu : p.nl;
+    Vector rv(const_cast<double *>(rhs), nsz);
+    LinearSolver solver(nsz, form == 0 ? p.m : p.t, hd->opt,
+                        form == 0 ? p.cell_metric : p.trace_metric);
+    if (hd->opt.precond == "block-ilu0") solver.Prepare(p.SolverGraph(form == 1), hd->opt);
+    LinearResult lr;
+    lr.x.SetSize(nsz);
+    lr.equation_residual.SetSize(nsz);
+    if (form == 0) {
+      Vector uv(const_cast<double *>(u), p.nu);
+      auto op = p.PartialDG(uv);
+      solver.Solve(*op, rv, hd->opt, lr);
+    } else {
+      solver.Solve(*hd->s.op, rv, hd->opt, lr);
+    }
+    std::memcpy(x, lr.x.GetData(), sizeof(double) * nsz);
+    std::memcpy(eq_residual, lr.equation_residual.GetData(), sizeof(double) * nsz);
+    *count = lr.count;
+    *relres = lr.residual;
+  });
+}
+}
