@@ -1,0 +1,275 @@
+/*
+ * euler2d_cuda.h -- C-ABI of the B200 (sm_100a) Newton-update engine for the
+ * frozen-HLL DG / condensed-HDG 2-D Euler solver of YueWu2002/mfem_euler2d_cpp.
+ *
+ * The reference has no FFI; its seams are C++ classes in include/euler.hpp.
+ * Every entry point below names the reference function it replaces, so a
+ * maintainer can route `--device cuda` through this library from the
+ * reference's Run() (src/stepper.cpp:28) without touching its CPU path.
+ *
+ * Conventions
+ *  - Every call returns an int status: EG_OK (0) or one of the EG_ERR_* codes,
+ *    which map 1:1 to the reference's require() messages (eg_status_string()).
+ *    No C++ exception, device trap or unbounded wait crosses this boundary.
+ *  - A context owns all device memory of one problem instance and one CUDA
+ *    stream; it is not thread-safe. Separate contexts are independent.
+ *  - Vector arguments may be host or device pointers (the library copies with
+ *    unified addressing). Layouts are the reference's (include/euler.hpp:44-45):
+ *    body  u[e*m + 4*i + c]  (cell e, native GL node i, component c),
+ *    trace l[f*t + 4*j + c]  (periodic face f, face GL node j, component c),
+ *    with q = k+1, p = q*q, m = 4p, t = 4q, n = nx*ny, nf = 2n.
+ *  - Cells are numbered row-major (e = iy*nx + ix); face 2e is the x-face
+ *    between e and its +x neighbour, face 2e+1 the y-face between e and its
+ *    +y neighbour (src/problem.cpp:77-90).
+ */
+#ifndef EULER2D_CUDA_H
+#define EULER2D_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EG_MAX_Q 9 /* k <= 8 (src/options.cpp:97) */
+#define EG_MAX_P (EG_MAX_Q * EG_MAX_Q)
+
+/* ------------------------------------------------------------ status codes */
+enum eg_status {
+  EG_OK = 0,
+  EG_ERR_INVALID = 1,           /* invalid argument or unsupported configuration */
+  EG_ERR_CUDA = 2,              /* CUDA runtime failure (text in eg_last_error) */
+  EG_ERR_NONPOSITIVE_FACE = 3,  /* "Nonpositive old face state; refine mesh" physics.cpp:46-49 */
+  EG_ERR_ROE_SOUND = 4,         /* "Invalid Roe sound speed" physics.cpp:58 */
+  EG_ERR_DEGENERATE_HLL = 5,    /* "Degenerate HLL speeds" problem.cpp:369 */
+  EG_ERR_INADMISSIBLE = 6,      /* "Old state is inadmissible; refine mesh" problem.cpp:353 */
+  EG_ERR_SINGULAR_CELL = 7,     /* "Singular streaming HDG cell factor" condensation.cpp:137 */
+  EG_ERR_SINGULAR_JACOBI = 8,   /* "Singular block Jacobi factor" linear.cpp:201 */
+  EG_ERR_SINGULAR_ILU = 9,      /* "Singular BSR ILU diagonal" block_ilu.cpp:84 */
+  EG_ERR_GMRES_BREAKDOWN = 10,  /* "GMRES Arnoldi breakdown" linear.cpp:129 */
+  EG_ERR_GMRES_NONFINITE = 11,  /* "Nonfinite GMRES residual" linear.cpp:152 */
+  EG_ERR_GMRES_LIMIT = 12,      /* "GMRES iteration limit reached" linear.cpp:155 */
+  EG_ERR_LINEAR_RESIDUAL = 13,  /* "True inverse-mass weighted linear residual too large" linear.cpp:246 */
+  EG_ERR_RECOVERED = 14,        /* "Recovered DG residual criterion failed after Schur refinement" stepper.cpp:180 */
+  EG_ERR_DG_LINEAR = 15,        /* "DG Newton linear residual too large" stepper.cpp:183 */
+  EG_ERR_LINE_SEARCH = 16,      /* "Newton line search failed" stepper.cpp:217 */
+  EG_ERR_OUT_OF_MEMORY = 17,    /* device allocation failed */
+  EG_ERR_STEP_INTERVAL = 18,    /* "Step leaves the smooth simple-wave interval ..." stepper.cpp:94-95 */
+  EG_ERR_NEWTON_CONVERGE = 19,  /* "Newton failed to converge" stepper.cpp:241 */
+  EG_ERR_DIRK_INADMISSIBLE = 20,/* "SSP-DIRK3 step produced an inadmissible state" stepper.cpp:251 */
+  EG_ERR_INITIAL = 21,          /* "Initial projection not positive; refine mesh" stepper.cpp:32 */
+  EG_ERR_UPDATE_EQUATION = 22,  /* "Independent recovered DG equation check failed" stepper.cpp:190 */
+  EG_ERR_UPDATE_EQUIVALENCE = 23, /* "DG/HDG one-update equivalence failed" stepper.cpp:197 */
+  EG_ERR_COUNT = 24
+};
+
+enum eg_form { EG_FORM_DG = 0, EG_FORM_HDG = 1 };
+enum eg_precond { EG_PC_BLOCK_JACOBI = 0, EG_PC_BLOCK_ILU0 = 1 };
+enum eg_assembly { EG_ASSEMBLY_PARTIAL = 0, EG_ASSEMBLY_FULL = 1 };
+enum eg_precision {
+  EG_PRECISION_FP64 = 0,  /* everything FP64 (parity path) */
+  EG_PRECISION_MIXED = 1  /* FP32 preconditioner + FP32 inner Schur GMRES in FP64 refinement */
+};
+
+/* Named device vectors of a context (eg_upload / eg_download). */
+enum eg_slot {
+  EG_SLOT_U = 0,       /* Newton state (nu) */
+  EG_SLOT_OLD = 1,     /* stage base / old state (nu) */
+  EG_SLOT_R = 2,       /* stored residual M^{-1} r_w + u - old (nu) */
+  EG_SLOT_DU = 3,      /* last Newton increment (nu) */
+  EG_SLOT_RHS = 4,     /* condensed Schur right-hand side (nl) */
+  EG_SLOT_LAMBDA = 5,  /* last Schur solution (nl) */
+  EG_SLOT_D = 6,       /* HDG trace diagonal D (nl) */
+  EG_SLOT_X = 7,       /* HDG responses X, n blocks of m x 4t column-major */
+  EG_SLOT_Y = 8,       /* HDG particular responses y (nu) */
+  EG_SLOT_PC_BLOCKS = 9, /* preconditioner blocks (DG: n*m*m, HDG: nf*t*t), column-major */
+  EG_SLOT_HLL_A = 10,  /* frozen left HLL bound per face point (nf*q) */
+  EG_SLOT_HLL_B = 11,  /* frozen right HLL bound per face point (nf*q) */
+  EG_SLOT_COUNT = 12
+};
+
+/* Problem description: geometry and the reference's host-computed tables
+ * (src/problem.cpp:32-222). Fixed-size arrays hold q <= EG_MAX_Q. */
+typedef struct eg_desc {
+  int nx, ny, k;
+  double gamma;        /* EulerGas gamma (src/main.cpp:8 uses 3) */
+  double safety;       /* HLL safety factor (Options::safety) */
+  double alpha;        /* wave angle in radians */
+  double lx, ly, hx, hy, area;
+  double w[EG_MAX_P];        /* volume GL weights, native node order */
+  double ew[EG_MAX_Q];       /* edge GL weights */
+  double ex[EG_MAX_Q];       /* edge GL points in [0,1] */
+  double inv_mass[EG_MAX_P]; /* diagonal of Problem::inv_mass */
+  double mass[EG_MAX_P];     /* diagonal of Problem::mass */
+  double tensor_dx[EG_MAX_P]; /* Problem::tensor_dx(a,i) at [a*q+i] */
+  double tensor_dy[EG_MAX_P]; /* Problem::tensor_dy(a,j) at [a*q+j] */
+  /* fv[s](j, node) along the normal line through face point j of side s:
+   * [(s*q + j)*q + l], node = j*q+l for s<2 and l*q+j for s>=2. */
+  double face_basis[4 * EG_MAX_Q * EG_MAX_Q];
+  int tensor_node[EG_MAX_P]; /* lexicographic -> native; must be the identity */
+} eg_desc;
+
+/* Solver options (the numerical subset of euler::Options, include/euler.hpp:46-57). */
+typedef struct eg_opts {
+  int form;        /* eg_form */
+  int precond;     /* eg_precond */
+  int assembly;    /* eg_assembly */
+  int precision;   /* eg_precision */
+  int restart;     /* GMRES restart (default 20) */
+  int max_krylov;  /* GMRES iteration limit (default 1500) */
+  double linear_tol; /* default 1e-12 */
+  int check_update;  /* HDG: independent DG solve of every update (stepper.cpp:184-201) */
+} eg_opts;
+
+/* Per-update statistics: the numeric columns of _iterations.csv
+ * (src/stepper.cpp:229-239). Times are seconds. */
+typedef struct eg_update_stats {
+  double residual_norm;  /* CellNorm(residual) before the update */
+  double damping;
+  int krylov_iterations;
+  int attempts;          /* Schur refinement attempts (HDG) */
+  double linear_relative_residual;
+  double dg_linear_relative_residual;
+  double residual_s, validation_s, jacobian_s, condensation_s, assembly_s, setup_s,
+      solve_s, recovery_s, line_search_s, iteration_s;
+  double device_ms;      /* CUDA-event time of the whole update on the context stream */
+  double update_check;   /* --check-update relative difference, -1 when not run */
+} eg_update_stats;
+
+/* Linear-solve statistics (LinearResult, include/euler.hpp:232-236). */
+typedef struct eg_linear_stats {
+  int count;
+  double residual;  /* relative weighted residual */
+  double rhs_norm;
+} eg_linear_stats;
+
+typedef struct eg_ctx eg_ctx;
+
+/* ---------------------------------------------------------------- setup */
+/* Fill a descriptor for the rotated simple-wave problem on an nx x ny periodic
+ * Qk mesh, computing the Gauss-Legendre tables on the host exactly as the
+ * reference Problem constructor does (src/problem.cpp:32-222). */
+int eg_desc_simple_wave(eg_desc *d, int nx, int ny, int k, double alpha_deg, double gamma,
+                        double safety);
+void eg_opts_default(eg_opts *o);
+
+/* Replaces: Problem construction + PrepareHybrid + LinearSolver construction
+ * (src/problem.cpp:32, src/condensation.cpp:47, src/linear.cpp:159). */
+int eg_create(const eg_desc *d, const eg_opts *o, eg_ctx **out);
+void eg_destroy(eg_ctx *ctx);
+/* Message of the last failure on ctx; with ctx == NULL, of the last failed
+ * eg_create on the calling thread. */
+const char *eg_last_error(const eg_ctx *ctx);
+const char *eg_status_string(int status);
+/* cudaStream_t of the context, as void*. */
+void *eg_stream(eg_ctx *ctx);
+/* Change solver options between updates (form, preconditioner, tolerance). */
+int eg_set_opts(eg_ctx *ctx, const eg_opts *o);
+/* Sizes: n, p, m, t, nf, nu, nl. */
+int eg_sizes(const eg_ctx *ctx, int out[7]);
+/* Device bytes held by the context. */
+long long eg_device_bytes(const eg_ctx *ctx);
+
+/* --------------------------------------------------------- state access */
+int eg_upload(eg_ctx *ctx, int slot, const double *src);
+int eg_download(eg_ctx *ctx, int slot, double *dst);
+/* Replaces: Problem::Initial (src/problem.cpp:329), L2 projection of the exact
+ * wave at t=0 into EG_SLOT_U (host computation, uploaded). */
+int eg_initial(eg_ctx *ctx);
+
+/* ---------------------------------------------------- operators (parity) */
+/* Replaces: Problem::Freeze (src/problem.cpp:350) at EG_SLOT_U, including
+ * old = u and dt = stage_dt; writes WaveRate (problem.cpp:377) if non-null. */
+int eg_freeze(eg_ctx *ctx, double stage_dt, int check_admissible, double *wave_rate);
+/* Sets Problem::dt (used after Freeze by the time loop, stepper.cpp:109). */
+int eg_set_dt(eg_ctx *ctx, double dt);
+/* Replaces: Problem::Residual (src/problem.cpp:445): EG_SLOT_R <- r(EG_SLOT_U). */
+int eg_residual(eg_ctx *ctx);
+/* Replaces: Problem::CellNorm (src/problem.cpp:385) of a body slot. */
+int eg_cell_norm(eg_ctx *ctx, int slot, double *out);
+/* Replaces: Problem::Admissible (src/problem.cpp:259) of a body slot. */
+int eg_admissible(eg_ctx *ctx, int slot, int *ok);
+/* Replaces: PartialDGOperator::Refresh + Mult (src/partial.cpp:31-135):
+ * y = J(EG_SLOT_U) x, nu-vectors. */
+int eg_dg_apply(eg_ctx *ctx, const double *x, double *y);
+/* Replaces: Problem::StreamCondense (src/condensation.cpp:131) at EG_SLOT_U
+ * with residual EG_SLOT_R: fills X, y, D and the Schur right-hand side. */
+int eg_condense(eg_ctx *ctx);
+/* Replaces: ElementOperator::Mult with borrowed factors (src/operators.cpp:147):
+ * Schur action y = D v - sum_e C_e X_e v_e, nl-vectors. */
+int eg_schur_apply(eg_ctx *ctx, const double *v, double *y);
+/* Replaces: Problem::Recover (src/condensation.cpp:154): du = -X lam - y. */
+int eg_recover(eg_ctx *ctx, const double *lam, double *du);
+/* Replaces: the preconditioner refresh in LinearSolver::Solve
+ * (src/linear.cpp:186-203): DiagonalBlocks+LU or FillBlocks+ILU factor for the
+ * current form. factor=0 stops after building (for EG_SLOT_PC_BLOCKS parity). */
+int eg_pc_factor(eg_ctx *ctx, int factor);
+/* Replaces: LinearSolver::Impl::Precondition (src/linear.cpp:66). */
+int eg_pc_apply(eg_ctx *ctx, const double *b, double *x);
+/* Replaces: LinearSolver::Solve (src/linear.cpp:167) for the current form:
+ * weighted right-preconditioned restarted CGS2 GMRES. x is in/out (used as
+ * the initial guess when refresh == 0); eq_residual (may be null) receives
+ * op*x - rhs. */
+int eg_linear_solve(eg_ctx *ctx, const double *rhs, double *x, double *eq_residual,
+                    int refresh, double linear_tol, eg_linear_stats *st);
+
+/* ------------------------------------------------------- Newton / stages */
+/* Stage setup (src/stepper.cpp:99-110): dt = stage_dt and EG_SLOT_OLD
+ * already uploaded or set; marks the stored residual stale. */
+int eg_stage_begin(eg_ctx *ctx, double stage_dt);
+/* Newton residual (stepper.cpp:118-121): recomputes EG_SLOT_R unless the last
+ * accepted line-search residual is still valid; returns CellNorm(r). */
+int eg_newton_residual(eg_ctx *ctx, double *residual_norm);
+/* One accepted damped Newton update (src/stepper.cpp:129-228), DG or HDG per
+ * the context's form: Jacobian / condensation, PC, GMRES, recovery and the
+ * recovered-residual refinement loop, validation and line search, all on the
+ * device. old_norm = CellNorm(stage base). */
+int eg_newton_update(eg_ctx *ctx, double residual_norm, double old_norm, eg_update_stats *st);
+
+/* --------------------------------------------------------- diagnostics */
+/* Replaces: Problem::Integral (src/problem.cpp:727) of EG_SLOT_U. */
+int eg_integral(eg_ctx *ctx, double out[4]);
+/* Replaces: Problem::Errors (src/problem.cpp:704) of EG_SLOT_U at time t. */
+int eg_errors(eg_ctx *ctx, double time, double out[4]);
+/* Replaces: Problem::Differences (src/problem.cpp:739): L2 norms of u - v per
+ * component for two host body vectors of the described problem. */
+int eg_differences(const eg_desc *d, const double *u, const double *v, double out[4]);
+
+/* ------------------------------------------------------------ time loop */
+/* Run options: the time-loop subset of euler::Options. */
+typedef struct eg_run_opts {
+  int integrator;     /* 0 = ssp-dirk3, 1 = be */
+  int steps;          /* > 0: fixed step count; else run to T */
+  int newton_steps;   /* > 0: fixed updates per stage; else converge */
+  int max_newton;
+  double dt, cfl, end, tol;
+  int timing_only, save_solution;
+  const char *prefix; /* output prefix, e.g. "<output>_dg" */
+  const char *form_name; /* "dg" or "hdg" for CSV rows */
+  /* echoed into _summary.csv */
+  const char *assembly_name, *solver_name, *precond_name, *ilu_ordering_name;
+  int check_update;
+} eg_run_opts;
+
+typedef struct eg_run_result {
+  double errors[4];
+  double seconds, drift, newton_seconds, final_time, mean_newton_s;
+  double newton_device_ms; /* sum of per-update CUDA-event times */
+  int updates, time_steps;
+} eg_run_result;
+
+/* Replaces: euler::Run (src/stepper.cpp:28-292), writing the same
+ * _iterations.csv / _summary.csv columns. The final state stays in EG_SLOT_U. */
+int eg_run(eg_ctx *ctx, const eg_run_opts *ro, eg_run_result *res);
+
+/* Incremental time loop for benchmarks: advances the SSP-DIRK3/BE schedule by
+ * exactly one accepted Newton update per call (stage and step transitions,
+ * Freeze and DIRK combination are performed between updates, outside the
+ * update's timed boundary). */
+typedef struct eg_stepper eg_stepper;
+int eg_stepper_create(eg_ctx *ctx, const eg_run_opts *ro, eg_stepper **out);
+int eg_stepper_next(eg_stepper *s, eg_update_stats *st);
+void eg_stepper_destroy(eg_stepper *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EULER2D_CUDA_H */

@@ -1,0 +1,390 @@
+// Cell-local kernels of the DG discretisation: frozen HLL bounds, admissibility,
+// the weak residual and its partially assembled Jacobian action (one fused
+// sum-factorised kernel), and the DG block-Jacobi build/factor/apply.
+//
+// Data layout (device): body vectors u[e*m + 4*i + c] with cells row-major and
+// nodes lexicographic; one thread owns one (cell, node) and its 4 components.
+// Neighbour traces are read straight from global memory (L1/L2 resident: each
+// cell's lines are re-read by at most its four neighbours), so no face buffer
+// round trip through HBM is needed.
+#include "eg_cellmat.cuh"
+#include "eg_internal.h"
+
+namespace eg {
+
+template <int Q>
+struct CellCfg {
+  static constexpr int P = Q * Q;
+  static constexpr int M = 4 * P;
+  static constexpr int CPB = (256 / P) < 64 ? (256 / P) : 64;  // cells per block
+  static constexpr int THREADS = CPB * P;
+};
+
+// ------------------------------------------------------------------ Freeze
+// One thread per face point (src/problem.cpp:357-374 and WaveRate 377-384).
+template <int Q>
+__global__ void __launch_bounds__(256) freeze_kernel(Geo g, const double *__restrict__ tab,
+                                                     const double *__restrict__ u, double *fa,
+                                                     double *fb, double *flw, double *frw,
+                                                     double *fpen, double *D, int *err,
+                                                     unsigned long long *wave) {
+  __shared__ STab<Q> st;
+  __shared__ double red[256];
+  load_tables<Q>(st, tab);
+  __syncthreads();
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  double speed = 0.;
+  if (idx < g.nf * Q) {
+    const int f = idx / Q, j = idx % Q, c = f >> 1, axis = f & 1;
+    const int R = neighbour(c, axis == 0 ? 1 : 3, g.nx, g.ny);
+    double ul[4], ur[4];
+    trace4<Q>(st, u, c, axis == 0 ? 1 : 3, j, ul);
+    trace4<Q>(st, u, R, axis == 0 ? 0 : 2, j, ur);
+    double a = 0., b = 0.;
+    const int code = hll_speeds(ul, ur, axis, g.gamma, g.gm1, g.safety, a, b);
+    if (code != DERR_NONE) {
+      raise_err(err, code);
+    } else if (!(a + b > 0)) {
+      raise_err(err, DERR_DEGENERATE_HLL);
+    }
+    const double inv = 1. / (a + b);
+    fa[idx] = a;
+    fb[idx] = b;
+    flw[idx] = b * inv;
+    frw[idx] = a * inv;
+    fpen[idx] = a * b * inv;
+    if (D) {
+      const double diag = st.ew(j) * (a + b);
+      double *dd = D + (size_t)f * (4 * Q) + 4 * j;
+      dd[0] = dd[1] = dd[2] = dd[3] = diag;
+    }
+    speed = fmax(a, b);
+  }
+  red[threadIdx.x] = speed;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  // non-negative doubles order like their bit patterns
+  if (threadIdx.x == 0) atomicMax(wave, (unsigned long long)__double_as_longlong(red[0]));
+}
+
+// ------------------------------------------------------------- Admissible
+// Positivity at every volume node and face point (src/problem.cpp:259-275).
+template <int Q>
+__global__ void __launch_bounds__(256) admissible_kernel(Geo g, const double *__restrict__ tab,
+                                                         const double *__restrict__ u, int *flag) {
+  using C = CellCfg<Q>;
+  __shared__ STab<Q> st;
+  load_tables<Q>(st, tab);
+  __syncthreads();
+  const int lc = threadIdx.x / C::P, node = threadIdx.x % C::P;
+  const int e = blockIdx.x * C::CPB + lc;
+  if (lc >= C::CPB || e >= g.n) return;
+  bool ok = true;
+  {
+    const double *v = u + (size_t)e * C::M + 4 * node;
+    const double s[4] = {v[0], v[1], v[2], v[3]};
+    ok = positive(s, g.gm1);
+  }
+  for (int task = node; task < 4 * Q; task += C::P) {
+    double s[4];
+    trace4<Q>(st, u, e, task / Q, task % Q, s);
+    ok = ok && positive(s, g.gm1);
+  }
+  if (!ok) *flag = 0;
+}
+
+// -------------------------------------------- residual / Jacobian action
+// MODE 0: r = M^{-1}[-dt sum_q w (Gx F_x + Gy F_y) + lifted HLL fluxes] + u - old
+//         (Problem::Residual, src/problem.cpp:445-507);
+// MODE 1: y = x + M^{-1}[-D_x^T(dt w J_x x) - D_y^T(dt w J_y x) + face lift of
+//         (lw J(U_L) + pen) x_L + (rw J(U_R) - pen) x_R]
+//         (PartialDGOperator::Mult, src/partial.cpp:62-135), with the flux
+//         Jacobians recomputed from the Newton state instead of cached.
+template <int Q, int MODE>
+__global__ void __launch_bounds__(CellCfg<Q>::THREADS)
+    cell_operator_kernel(Geo g, const double *__restrict__ tab, Frozen fz,
+                         const double *__restrict__ u, const double *__restrict__ x_or_old,
+                         double *__restrict__ out) {
+  using C = CellCfg<Q>;
+  constexpr int P = C::P, M = C::M, CPB = C::CPB;
+  __shared__ STab<Q> st;
+  __shared__ double fxs[CPB][P][4], fys[CPB][P][4];
+  __shared__ double hs[CPB][4 * Q][4];
+  load_tables<Q>(st, tab);
+  __syncthreads();
+  const int lc = threadIdx.x / P, node = threadIdx.x % P;
+  const int e = blockIdx.x * CPB + lc;
+  const bool active = lc < CPB && e < g.n;
+  double uu[4] = {0., 0., 0., 0.}, xx[4] = {0., 0., 0., 0.};
+  if (active) {
+    const double *v = u + (size_t)e * M + 4 * node;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) uu[c] = v[c];
+    const double *xv = x_or_old + (size_t)e * M + 4 * node;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) xx[c] = xv[c];
+    const double wdt = g.dt * st.w(node);
+    double fx[4], fy[4];
+    if (MODE == 0) {
+      flux(uu, 0, g.gm1, fx);
+      flux(uu, 1, g.gm1, fy);
+    } else {
+      double j[16];
+      jacobian(uu, 0, g.gm1, j);
+      mat4_vec(j, xx, fx);
+      jacobian(uu, 1, g.gm1, j);
+      mat4_vec(j, xx, fy);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      fxs[lc][node][c] = wdt * fx[c];
+      fys[lc][node][c] = wdt * fy[c];
+    }
+  }
+  if (lc < CPB && e < g.n) {
+    for (int task = node; task < 4 * Q; task += P) {
+      const int s = task / Q, j = task % Q;
+      const bool own_left = side_is_left(s);
+      const int nb = neighbour(e, s, g.nx, g.ny);
+      const int cl = own_left ? e : nb, cr = own_left ? nb : e;
+      const int sl = s < 2 ? 1 : 3, sr = sl - 1;
+      const int axis = s < 2 ? 0 : 1;
+      const int f = own_left ? 2 * e + axis : 2 * nb + axis;
+      const int fi = f * Q + j;
+      double ul[4], ur[4], h[4];
+      trace4<Q>(st, u, cl, sl, j, ul);
+      trace4<Q>(st, u, cr, sr, j, ur);
+      const double lw = fz.lw[fi], rw = fz.rw[fi], pen = fz.pen[fi];
+      if (MODE == 0) {
+        double fl[4], fr[4];
+        flux(ul, axis, g.gm1, fl);
+        flux(ur, axis, g.gm1, fr);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) h[c] = lw * fl[c] + rw * fr[c] + pen * (ul[c] - ur[c]);
+      } else {
+        double xl[4], xr[4], jl[16], jr[16], zl[4], zr[4];
+        trace4<Q>(st, x_or_old, cl, sl, j, xl);
+        trace4<Q>(st, x_or_old, cr, sr, j, xr);
+        jacobian(ul, axis, g.gm1, jl);
+        jacobian(ur, axis, g.gm1, jr);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          jl[k] *= lw;
+          jr[k] *= rw;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          jl[c * 5] += pen;
+          jr[c * 5] -= pen;
+        }
+        mat4_vec(jl, xl, zl);
+        mat4_vec(jr, xr, zr);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) h[c] = zl[c] + zr[c];
+      }
+      const double len = axis == 0 ? g.hy : g.hx;
+      const double scale = g.dt * len / g.area * st.ew(j);
+      const double sg = own_left ? scale : -scale;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) hs[lc][task][c] = sg * h[c];
+    }
+  }
+  __syncthreads();
+  if (!active) return;
+  const int ix = node % Q, iy = node / Q;
+  double acc[4] = {0., 0., 0., 0.};
+#pragma unroll
+  for (int a = 0; a < Q; ++a) {
+    const double dx = st.tdx(a, ix), dy = st.tdy(a, iy);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c] += dx * fxs[lc][iy * Q + a][c] + dy * fys[lc][a * Q + ix][c];
+  }
+  const double w0 = st.fb(0, iy, ix), w1 = st.fb(1, iy, ix);
+  const double w2 = st.fb(2, ix, iy), w3 = st.fb(3, ix, iy);
+  const double im = st.inv_mass(node);
+  double *o = out + (size_t)e * M + 4 * node;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double face = w0 * hs[lc][0 * Q + iy][c] + w1 * hs[lc][1 * Q + iy][c] +
+                        w2 * hs[lc][2 * Q + ix][c] + w3 * hs[lc][3 * Q + ix][c];
+    const double v = im * (face - acc[c]);
+    o[c] = MODE == 0 ? v + uu[c] - xx[c] : v + xx[c];
+  }
+}
+
+template <int Q>
+__host__ __device__ constexpr int lu_rmax() {
+  return (4 * Q * Q + 31) / 32;
+}
+// Cells whose m x m block (plus staging) fits in shared memory.
+template <int Q>
+__host__ __device__ constexpr bool dg_block_in_smem() {
+  return 4 * Q * Q <= 144;
+}
+
+// ------------------------------------------------------ DG block Jacobi
+// Per cell: diagonal block (volume + own-face HLL terms) built at the Newton
+// state, then factored in place with partial pivoting (linear.cpp:198-202).
+template <int Q>
+__global__ void __launch_bounds__(256)
+    dg_jacobi_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                     double *blocks, int *pivots, bool factor, int *err) {
+  constexpr int P = Q * Q, M = 4 * P;
+  constexpr bool SM = dg_block_in_smem<Q>();
+  __shared__ STab<Q> st;
+  __shared__ double us[M], UT[16 * Q], FM[4 * Q * 16];
+  __shared__ int piv_s[M];
+  __shared__ double inv_piv[M];
+  __shared__ double bcast[2];
+  extern __shared__ double dyn[];
+  load_tables<Q>(st, tab);
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < M; i += blockDim.x) us[i] = u[(size_t)e * M + i];
+    __syncthreads();
+    cell_traces<Q>(st, us, UT);
+    __syncthreads();
+    // DG face matrices: own-left sides add lw J(U_L) + pen I, own-right sides
+    // subtract rw J(U_R) - pen I (src/partial.cpp:272-294).
+    for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
+      const int s = task / Q, j = task % Q;
+      const bool L = side_is_left(s);
+      const int f = cell_face(e, s, g.nx, g.ny);
+      const int fi = f * Q + j;
+      double jm[16];
+      jacobian(UT + 4 * task, s < 2 ? 0 : 1, g.gm1, jm);
+      const double wgt = L ? fz.lw[fi] : fz.rw[fi], pen = fz.pen[fi];
+      double *fm = FM + task * 16;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const bool diag = (k % 5) == 0;
+        const double v = wgt * jm[k] + (diag ? (L ? pen : -pen) : 0.);
+        fm[k] = L ? v : -v;
+      }
+    }
+    __syncthreads();
+    double *A = SM ? dyn : blocks + (size_t)e * M * M;
+    build_cell_matrix<Q>(A, M, st, us, FM, g);
+    __syncthreads();
+    if (factor) {
+      const bool ok = cta_lu_solve<lu_rmax<Q>()>(A, M, nullptr, 1, M, 0, piv_s, inv_piv, bcast);
+      if (!ok && threadIdx.x == 0) raise_err(err, DERR_SINGULAR_JACOBI);
+    } else {
+      for (int i = threadIdx.x; i < M; i += blockDim.x) piv_s[i] = i;
+    }
+    __syncthreads();
+    if (SM) {
+      double *dst = blocks + (size_t)e * M * M;
+      for (int i = threadIdx.x; i < M * M; i += blockDim.x) dst[i] = A[i];
+    }
+    for (int i = threadIdx.x; i < M; i += blockDim.x) pivots[(size_t)e * M + i] = piv_s[i];
+  }
+}
+
+// --------------------------------------------------------- block LU apply
+// x_b = LU_b^{-1} b_b for every block (one warp per block); Jacobi apply of
+// LinearSolver::Impl::Precondition (src/linear.cpp:66-75).
+__global__ void __launch_bounds__(256) block_apply_kernel(const double *__restrict__ blocks,
+                                                          const int *__restrict__ piv, int nblocks,
+                                                          int bs, const double *__restrict__ b,
+                                                          double *__restrict__ x) {
+  extern __shared__ double xs[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int blk = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (blk >= nblocks) return;
+  double *v = xs + warp * bs;
+  for (int i = lane; i < bs; i += 32) v[i] = b[(size_t)blk * bs + i];
+  __syncwarp();
+  warp_lu_apply(blocks + (size_t)blk * bs * bs, piv + (size_t)blk * bs, bs, v);
+  for (int i = lane; i < bs; i += 32) x[(size_t)blk * bs + i] = v[i];
+}
+
+// ================================================================ launchers
+static Frozen frozen_of(Ctx &c) { return Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}; }
+
+void launch_freeze(Ctx &c, const double *u, bool check_admissible) {
+  if (check_admissible) {
+    launch_admissible(c, u);
+    c.sync();
+    int ok = 1;
+    EG_CUDA(cudaMemcpy(&ok, c.derr + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!ok) fail(EG_ERR_INADMISSIBLE, "Old state is inadmissible; refine mesh");
+  }
+  EG_CUDA(cudaMemsetAsync(c.dscal + DS_WAVE, 0, sizeof(double), c.stream));
+  const int total = c.nf * c.q;
+  const int blocks = (total + 255) / 256;
+  EG_DISPATCH_Q(c.q, freeze_kernel<Q><<<blocks, 256, 0, c.stream>>>(
+                         c.geo, c.tab, u, c.fa, c.fbb, c.flw, c.frw, c.fpen, c.D, c.derr,
+                         reinterpret_cast<unsigned long long *>(c.dscal + DS_WAVE)));
+  EG_CUDA(cudaGetLastError());
+}
+
+void launch_admissible(Ctx &c, const double *u) {
+  const int one = 1;
+  EG_CUDA(cudaMemcpyAsync(c.derr + 1, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  EG_DISPATCH_Q(c.q, {
+    using C = CellCfg<Q>;
+    const int blocks = (c.n + C::CPB - 1) / C::CPB;
+    admissible_kernel<Q><<<blocks, C::THREADS, 0, c.stream>>>(c.geo, c.tab, u, c.derr + 1);
+  });
+  EG_CUDA(cudaGetLastError());
+}
+
+void launch_residual(Ctx &c, const double *u, const double *old, double *r) {
+  EG_DISPATCH_Q(c.q, {
+    using C = CellCfg<Q>;
+    const int blocks = (c.n + C::CPB - 1) / C::CPB;
+    cell_operator_kernel<Q, 0><<<blocks, C::THREADS, 0, c.stream>>>(c.geo, c.tab, frozen_of(c), u,
+                                                                     old, r);
+  });
+  EG_CUDA(cudaGetLastError());
+}
+
+void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y) {
+  EG_DISPATCH_Q(c.q, {
+    using C = CellCfg<Q>;
+    const int blocks = (c.n + C::CPB - 1) / C::CPB;
+    cell_operator_kernel<Q, 1><<<blocks, C::THREADS, 0, c.stream>>>(c.geo, c.tab, frozen_of(c), u,
+                                                                     x, y);
+  });
+  EG_CUDA(cudaGetLastError());
+}
+
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+void launch_dg_jacobi(Ctx &c, const double *u, bool factor) {
+  c.ensure_pc_dg();
+  EG_DISPATCH_Q(c.q, {
+    constexpr int M = 4 * Q * Q;
+    const size_t dyn = dg_block_in_smem<Q>() ? sizeof(double) * M * M : 0;
+    auto kern = dg_jacobi_kernel<Q>;
+    if (dyn > 48 * 1024)
+      EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    const int grid = std::min(c.n, sm_count() * 8);
+    kern<<<grid, 256, dyn, c.stream>>>(c.geo, c.tab, frozen_of(c), u, c.pc_dg, c.piv_dg, factor, c.derr);
+  });
+  EG_CUDA(cudaGetLastError());
+}
+
+void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,
+                        const double *b, double *x) {
+  const int warps = 8;
+  const int grid = (nblocks + warps - 1) / warps;
+  const size_t dyn = sizeof(double) * bs * warps;
+  block_apply_kernel<<<grid, warps * 32, dyn, c.stream>>>(blocks, piv, nblocks, bs, b, x);
+  EG_CUDA(cudaGetLastError());
+}
+
+}  // namespace eg

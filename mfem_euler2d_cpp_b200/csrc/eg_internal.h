@@ -1,0 +1,173 @@
+// Host-side context of one problem instance and the kernel launchers shared
+// between translation units. Not part of the public C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/euler2d_cuda.h"
+#include "eg_device.cuh"
+
+#define EG_DISPATCH_Q(qv, ...)                   \
+  switch (qv) {                                  \
+    case 1: { constexpr int Q = 1; __VA_ARGS__; } break; \
+    case 2: { constexpr int Q = 2; __VA_ARGS__; } break; \
+    case 3: { constexpr int Q = 3; __VA_ARGS__; } break; \
+    case 4: { constexpr int Q = 4; __VA_ARGS__; } break; \
+    case 5: { constexpr int Q = 5; __VA_ARGS__; } break; \
+    case 6: { constexpr int Q = 6; __VA_ARGS__; } break; \
+    case 7: { constexpr int Q = 7; __VA_ARGS__; } break; \
+    case 8: { constexpr int Q = 8; __VA_ARGS__; } break; \
+    case 9: { constexpr int Q = 9; __VA_ARGS__; } break; \
+    default: break;                              \
+  }
+
+namespace eg {
+
+// Thrown inside the library only; converted to a status at the C-ABI.
+struct Failure {
+  int status;
+  std::string msg;
+};
+[[noreturn]] void fail(int status, const std::string &msg);
+void cuda_check(cudaError_t e, const char *what);
+#define EG_CUDA(call) ::eg::cuda_check((call), #call)
+
+// Fixed grid of the deterministic reductions (partials are summed in block
+// order by the last block to finish).
+constexpr int kRedBlocks = 296;
+constexpr int kRedThreads = 256;
+
+// Device scalar slots (doubles) used by reductions and control.
+enum DScal : int {
+  DS_NORM = 0,       // generic reduction result
+  DS_NORM2 = 1,
+  DS_WAVE = 2,       // max HLL speed bits (as unsigned long long)
+  DS_ADMISSIBLE = 3, // 1.0 when admissible
+  DS_COUNT = 8
+};
+
+// GMRES control block (device). Sized for restart R <= kMaxRestart.
+constexpr int kMaxRestart = 64;
+struct GmresCtl {
+  double h[(kMaxRestart + 1) * kMaxRestart];  // column-major (R+1) x R
+  double g[kMaxRestart + 1];
+  double cs[kMaxRestart], sn[kMaxRestart], y[kMaxRestart];
+  double proj[kMaxRestart + 1];
+  double next;         // norm of the orthogonalised Krylov vector
+  double inv_next;
+  double rhs_norm, tol, abs_tol;
+  int j, count, stop, err;
+};
+
+struct Ctx;
+
+// Operators used by the Krylov solver.
+struct LinearOps {
+  int N;
+  const double *mtab;  // metric table (device)
+  int period;          // metric period in entries
+  virtual void apply(Ctx &c, const double *x, double *y) = 0;
+  virtual void precondition(Ctx &c, const double *b, double *x) = 0;
+  virtual ~LinearOps() = default;
+};
+
+struct Ctx {
+  eg_desc desc{};
+  eg_opts opts{};
+  int q = 0, p = 0, m = 0, t = 0, n = 0, nf = 0, nu = 0, nl = 0;
+  Geo geo{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long bytes = 0;
+  std::vector<void *> allocations;
+
+  // tables and metrics
+  double *tab = nullptr;
+  double *mtab_dg = nullptr, *mtab_hdg = nullptr;
+  // body vectors (nu)
+  double *u = nullptr, *old = nullptr, *r = nullptr, *du = nullptr, *trial = nullptr,
+         *trial_r = nullptr, *er = nullptr, *tmp_body = nullptr;
+  // frozen HLL data (nf*q)
+  double *fa = nullptr, *fbb = nullptr, *flw = nullptr, *frw = nullptr, *fpen = nullptr;
+  // HDG (allocated lazily)
+  double *D = nullptr;     // nl
+  double *XY = nullptr;    // n*m*(4t+1): per cell [X (m x 4t) | y (m)]
+  double *Cb = nullptr;    // n*4q*16 restriction flux blocks C
+  double *sf = nullptr;    // n*4q lift scalars B
+  double *contrib = nullptr;  // n*4t per-cell face contributions
+  double *panels = nullptr;   // n*4*t*t Schur Jacobi panels
+  double *rhs = nullptr, *lam = nullptr, *tmp_trace = nullptr;  // nl
+  double *work_cell = nullptr;  // global LU workspace for large cells
+  int work_slots = 0;
+  // preconditioners (factored in place): DG n blocks m x m, HDG nf blocks t x t
+  double *pc_dg = nullptr, *pc_hdg = nullptr;
+  int *piv_dg = nullptr, *piv_hdg = nullptr;
+  // Krylov workspace (size N = max(nu, nl) so both forms share it)
+  int kN = 0, kR = 0;
+  double *V = nullptr;
+  double *kw = nullptr, *kz = nullptr, *kres = nullptr, *kcomb = nullptr, *kcorr = nullptr,
+         *kx = nullptr;
+  GmresCtl *ctl = nullptr;
+  GmresCtl *hctl = nullptr;  // pinned mirror
+  double *partials = nullptr;  // kRedBlocks * (kMaxRestart+1)
+  unsigned *counter = nullptr;
+  // error word (derr[0]) and admissibility flag (derr[1])
+  int *derr = nullptr;
+  double *dscal = nullptr;
+  double *hscal = nullptr;  // pinned mirror of dscal
+  int *herr = nullptr;      // pinned
+  // events for per-update device timing
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_residual_s = 0.;
+  bool update_timer_open = false;
+
+  bool residual_ready = false;
+  bool condensed = false;
+
+  void *alloc(size_t bytes);
+  template <class T>
+  T *alloc_n(size_t n) {
+    return static_cast<T *>(alloc(n * sizeof(T)));
+  }
+  void ensure_hdg();
+  void ensure_krylov();
+  void ensure_pc_dg();
+  void ensure_pc_hdg();
+  void sync();
+  void check_device_error();
+};
+
+// ---- launchers (eg_cell.cu) ----
+void launch_freeze(Ctx &c, const double *u, bool check_admissible);
+void launch_admissible(Ctx &c, const double *u);  // writes dscal[DS_ADMISSIBLE]
+void launch_residual(Ctx &c, const double *u, const double *old, double *r);
+void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y);
+void launch_dg_jacobi(Ctx &c, const double *u, bool factor);
+void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,
+                        const double *b, double *x);
+// ---- launchers (eg_hdg.cu) ----
+void launch_condense(Ctx &c, const double *u, const double *r);
+void launch_schur_apply(Ctx &c, const double *v, double *y);
+void launch_recover(Ctx &c, const double *lam, double *du);
+void launch_recovered_residual(Ctx &c, const double *eq, double *er);
+void launch_schur_jacobi(Ctx &c, bool factor);
+// ---- launchers (eg_krylov.cu) ----
+// Weighted squared norm sum(metric * x * x) into dscal[slot] (device).
+void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot);
+double wnorm(Ctx &c, const double *x, int N, const double *mtab, int period);
+void launch_axpby(Ctx &c, int N, double a, const double *x, double b, const double *y, double *out);
+void launch_copy(Ctx &c, int N, const double *x, double *out);
+void launch_fill(Ctx &c, int N, double v, double *out);
+double cell_norm(Ctx &c, const double *x);
+// Weighted restarted GMRES (src/linear.cpp:76-157). Returns the true residual
+// norm; sets *count. Throws Failure on breakdown / limit / non-finite.
+double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
+             bool zero_guess, int *count, double *rhs_norm_out);
+// ---- eg_api.cu ----
+// One accepted damped Newton update (src/stepper.cpp:129-228).
+void newton_update(Ctx &c, double residual_norm, double old_norm, eg_update_stats *st);
+
+}  // namespace eg

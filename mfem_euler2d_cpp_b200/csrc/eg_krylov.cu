@@ -1,0 +1,346 @@
+// Weighted vector algebra and restarted right-preconditioned CGS2 GMRES
+// (LinearSolver::Impl, src/linear.cpp:11-157), resident on the device.
+//
+// Every reduction runs on a fixed grid of kRedBlocks blocks; each block writes
+// its partial sums and the last block to finish adds the partials in block
+// order, so results are bitwise reproducible for a given size. The dual-norm
+// metric is not stored: it is periodic (cell metric |K| M_ii repeats every m
+// entries, trace metric len_f / ew_j every 2t entries) and is read from a
+// small table staged in shared memory.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+#include "eg_internal.h"
+
+namespace eg {
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// Returns true in the last block to finish (after all partials are visible).
+__device__ __forceinline__ bool last_block(unsigned *counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned ticket = atomicAdd(counter, 1u);
+    is_last = ticket == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+constexpr int kChunk = 8;  // Krylov columns per register chunk
+
+// ---------------------------------------------------------- weighted norm
+__global__ void __launch_bounds__(kRedThreads)
+    wnorm2_kernel(int N, const double *__restrict__ x, const double *__restrict__ mtab, int period,
+                  double *partials, unsigned *counter, double *out) {
+  __shared__ double red[kRedThreads];
+  __shared__ double mt[2 * EG_MAX_P];
+  for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
+  __syncthreads();
+  double s = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const double v = x[i];
+    s += mt[(i % period) >> 2] * v * v;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (last_block(counter)) {
+    double t = 0.;
+    for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += partials[b];
+    t = block_sum(t, red);
+    if (threadIdx.x == 0) {
+      *out = t;
+      *counter = 0;
+    }
+  }
+}
+
+// ------------------------------------------------------------ CGS2 passes
+// MODE 0: proj = V^T (metric w)                        (first pass)
+// MODE 1: w -= V proj_in; proj = V^T (metric w)        (second pass)
+// MODE 2: w -= V proj_in; next = ||w||_metric         (norm)
+// proj results are added into the Hessenberg column (h(i,j) += proj_i).
+template <int MODE>
+__global__ void __launch_bounds__(kRedThreads)
+    cgs_kernel(int N, double *__restrict__ w, const double *__restrict__ V, size_t ldv, int ncols,
+               const double *__restrict__ mtab, int period, double *partials, unsigned *counter,
+               GmresCtl *ctl, int R) {
+  __shared__ double red[kRedThreads];
+  __shared__ double mt[2 * EG_MAX_P];
+  __shared__ double pin[kMaxRestart + 1];
+  for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
+  if (MODE > 0)
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) pin[i] = ctl->proj[i];
+  __syncthreads();
+  const int stride = gridDim.x * blockDim.x;
+  const int j = ctl->j;
+  if (MODE == 2) {
+    double s = 0.;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+      double comb = 0.;
+      for (int c = 0; c < ncols; ++c) comb += V[c * ldv + i] * pin[c];
+      const double v = w[i] - comb;
+      w[i] = v;
+      s += mt[(i % period) >> 2] * v * v;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+    if (last_block(counter)) {
+      double t = 0.;
+      for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += partials[b];
+      t = block_sum(t, red);
+      if (threadIdx.x == 0) {
+        const double next = sqrt(t);
+        ctl->next = next;
+        ctl->inv_next = next > 0 ? 1. / next : 0.;
+        ctl->h[(j + 1) + (R + 1) * j] = next;
+        *counter = 0;
+      }
+    }
+    return;
+  }
+  if (MODE == 1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+      double comb = 0.;
+      for (int c = 0; c < ncols; ++c) comb += V[c * ldv + i] * pin[c];
+      w[i] -= comb;
+    }
+    // each thread re-reads only its own elements below: no grid barrier needed
+  }
+  for (int c0 = 0; c0 < ncols; c0 += kChunk) {
+    const int nc = min(kChunk, ncols - c0);
+    double acc[kChunk];
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) acc[k] = 0.;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+      const double wm = mt[(i % period) >> 2] * w[i];
+#pragma unroll
+      for (int k = 0; k < kChunk; ++k)
+        if (k < nc) acc[k] += V[(c0 + k) * ldv + i] * wm;
+    }
+    for (int k = 0; k < nc; ++k) {
+      const double s = block_sum(acc[k], red);
+      if (threadIdx.x == 0) partials[(size_t)(c0 + k) * gridDim.x + blockIdx.x] = s;
+    }
+  }
+  if (last_block(counter)) {
+    for (int c = 0; c < ncols; ++c) {
+      double t = 0.;
+      for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += partials[(size_t)c * gridDim.x + b];
+      t = block_sum(t, red);
+      if (threadIdx.x == 0) {
+        ctl->proj[c] = t;
+        ctl->h[c + (R + 1) * j] += t;
+      }
+    }
+    if (threadIdx.x == 0) *counter = 0;
+  }
+}
+
+// V_{j+1} = w * (1/next) when next > 0 (src/linear.cpp:119-122)
+__global__ void normalize_kernel(int N, const double *__restrict__ w, double *__restrict__ vnext,
+                                 const GmresCtl *ctl) {
+  const double next = ctl->next;
+  if (!(next > 0)) return;
+  const double s = 1. / next;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    vnext[i] = w[i] * s;
+}
+
+// Givens update of Hessenberg column j and the convergence test
+// (src/linear.cpp:123-136). Single thread.
+__global__ void givens_kernel(GmresCtl *ctl, int R) {
+  const int j = ctl->j;
+  double *h = ctl->h;
+  const int ld = R + 1;
+  for (int i = 0; i < j; ++i) {
+    const double u = h[i + ld * j], v = h[(i + 1) + ld * j];
+    h[i + ld * j] = ctl->cs[i] * u + ctl->sn[i] * v;
+    h[(i + 1) + ld * j] = -ctl->sn[i] * u + ctl->cs[i] * v;
+  }
+  const double d = hypot(h[j + ld * j], h[(j + 1) + ld * j]);
+  if (!(isfinite(d) && d > 0)) {
+    ctl->err = 1;
+    ctl->stop = 1;
+    return;
+  }
+  ctl->cs[j] = h[j + ld * j] / d;
+  ctl->sn[j] = h[(j + 1) + ld * j] / d;
+  h[j + ld * j] = d;
+  h[(j + 1) + ld * j] = 0.;
+  ctl->g[j + 1] = -ctl->sn[j] * ctl->g[j];
+  ctl->g[j] *= ctl->cs[j];
+  ctl->count = j + 1;
+  ctl->stop = (fabs(ctl->g[j + 1]) <= ctl->abs_tol || ctl->next <= DBL_MIN) ? 1 : 0;
+  ctl->j = j + 1;
+}
+
+// Upper-triangular solve for the Krylov coefficients (src/linear.cpp:138-142).
+__global__ void backsub_kernel(GmresCtl *ctl, int R) {
+  const int count = ctl->count, ld = R + 1;
+  for (int i = count - 1; i >= 0; --i) {
+    double v = ctl->g[i];
+    for (int k = i + 1; k < count; ++k) v -= ctl->h[i + ld * k] * ctl->y[k];
+    ctl->y[i] = v / ctl->h[i + ld * i];
+  }
+}
+
+__global__ void cycle_init_kernel(GmresCtl *ctl, int R, double beta, double abs_tol) {
+  for (int i = threadIdx.x; i < (R + 1) * R; i += blockDim.x) ctl->h[i] = 0.;
+  for (int i = threadIdx.x; i <= R; i += blockDim.x) ctl->g[i] = 0.;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctl->g[0] = beta;
+    ctl->j = 0;
+    ctl->count = 0;
+    ctl->stop = 0;
+    ctl->err = 0;
+    ctl->abs_tol = abs_tol;
+  }
+}
+
+// out = V[:, 0:count] y (src/linear.cpp:145-146)
+__global__ void combine_kernel(int N, const double *__restrict__ V, size_t ldv,
+                               const GmresCtl *__restrict__ ctl, double *__restrict__ out) {
+  __shared__ double ys[kMaxRestart];
+  const int count = ctl->count;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) ys[i] = ctl->y[i];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double s = 0.;
+    for (int c = 0; c < count; ++c) s += V[c * ldv + i] * ys[c];
+    out[i] = s;
+  }
+}
+
+__global__ void axpby_kernel(int N, double a, const double *__restrict__ x, double b,
+                             const double *__restrict__ y, double *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    out[i] = a * x[i] + b * y[i];
+}
+__global__ void scale_kernel(int N, double a, const double *__restrict__ x, double *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    out[i] = x[i] * a;
+}
+__global__ void sub_kernel(int N, const double *__restrict__ x, const double *__restrict__ y,
+                           double *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    out[i] = x[i] - y[i];
+}
+__global__ void add_kernel(int N, const double *__restrict__ x, double *__restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+__global__ void fill_kernel(int N, double v, double *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) out[i] = v;
+}
+
+static int vec_grid(int N) { return std::max(1, std::min((N + 255) / 256, 148 * 16)); }
+
+void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot) {
+  wnorm2_kernel<<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, x, mtab, period, c.partials, c.counter,
+                                                          c.dscal + slot);
+  EG_CUDA(cudaGetLastError());
+}
+double wnorm(Ctx &c, const double *x, int N, const double *mtab, int period) {
+  launch_wnorm2(c, x, N, mtab, period, DS_NORM);
+  EG_CUDA(cudaMemcpyAsync(c.hscal + DS_NORM, c.dscal + DS_NORM, sizeof(double),
+                          cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  return std::sqrt(c.hscal[DS_NORM]);
+}
+double cell_norm(Ctx &c, const double *x) { return wnorm(c, x, c.nu, c.mtab_dg, c.m); }
+
+void launch_axpby(Ctx &c, int N, double a, const double *x, double b, const double *y, double *out) {
+  axpby_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, a, x, b, y, out);
+  EG_CUDA(cudaGetLastError());
+}
+void launch_copy(Ctx &c, int N, const double *x, double *out) {
+  if (x != out)
+    EG_CUDA(cudaMemcpyAsync(out, x, sizeof(double) * N, cudaMemcpyDeviceToDevice, c.stream));
+}
+void launch_fill(Ctx &c, int N, double v, double *out) {
+  fill_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, v, out);
+  EG_CUDA(cudaGetLastError());
+}
+
+// -------------------------------------------------------------------- GMRES
+double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
+             bool zero_guess, int *count, double *rhs_norm_out) {
+  c.ensure_krylov();
+  const int N = ops.N;
+  const int R = std::min(N, c.kR);
+  const size_t ldv = (size_t)c.kN;
+  double *res = c.kres, *w = c.kw, *z = c.kz;
+  if (zero_guess) {
+    launch_fill(c, N, 0., x);
+    launch_copy(c, N, rhs, res);
+  } else {
+    ops.apply(c, x, w);
+    sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
+    EG_CUDA(cudaGetLastError());
+  }
+  const double rhs_norm = wnorm(c, rhs, N, ops.mtab, ops.period);
+  if (rhs_norm_out) *rhs_norm_out = rhs_norm;
+  *count = 0;
+  if (rhs_norm == 0.) return 0.;
+  int iterations = 0;
+  double residual_norm = wnorm(c, res, N, ops.mtab, ops.period);
+  while (iterations < limit) {
+    const double beta = residual_norm;
+    if (beta <= tol * rhs_norm) break;
+    scale_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, 1 / beta, res, c.V);
+    cycle_init_kernel<<<1, 256, 0, c.stream>>>(c.ctl, R, beta, tol * rhs_norm);
+    EG_CUDA(cudaGetLastError());
+    for (int j = 0; j < R && iterations < limit; ++j) {
+      const double *vj = c.V + (size_t)j * ldv;
+      ops.precondition(c, vj, z);
+      ops.apply(c, z, w);
+      const int nc = j + 1;
+      cgs_kernel<0><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
+                                                              c.partials, c.counter, c.ctl, R);
+      cgs_kernel<1><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
+                                                              c.partials, c.counter, c.ctl, R);
+      cgs_kernel<2><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
+                                                              c.partials, c.counter, c.ctl, R);
+      normalize_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, w, c.V + (size_t)(j + 1) * ldv, c.ctl);
+      givens_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
+      EG_CUDA(cudaGetLastError());
+      EG_CUDA(cudaMemcpyAsync(&c.hctl->stop, &c.ctl->stop, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                              c.stream));
+      c.sync();
+      ++iterations;
+      if (c.hctl->err) fail(EG_ERR_GMRES_BREAKDOWN, "GMRES Arnoldi breakdown");
+      if (c.hctl->stop) break;
+    }
+    backsub_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
+    combine_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.V, ldv, c.ctl, c.kcomb);
+    EG_CUDA(cudaGetLastError());
+    ops.precondition(c, c.kcomb, c.kcorr);
+    add_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.kcorr, x);
+    ops.apply(c, x, w);
+    sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
+    EG_CUDA(cudaGetLastError());
+    residual_norm = wnorm(c, res, N, ops.mtab, ops.period);
+    if (!std::isfinite(residual_norm)) fail(EG_ERR_GMRES_NONFINITE, "Nonfinite GMRES residual");
+  }
+  *count = iterations;
+  if (!(residual_norm <= tol * rhs_norm)) fail(EG_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+  return residual_norm;
+}
+
+}  // namespace eg

@@ -1,0 +1,256 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs only where the reference sources are available (it needs the oracle
+build in oracle/_ref/, made by `make -C oracle`): the unmodified reference
+compiled against the MFEM-subset shim. Two kinds of fixture are written:
+
+* units_*.npz  -- reference public API (Problem, PartialDG, StreamCondense,
+  Schur operator, Recover, LinearSolver) on small meshes for k = 0..8: the
+  frozen HLL bounds, residual, Jacobian action, block-Jacobi blocks,
+  condensation (X, y, rhs, D), Schur action and blocks, recovery and one
+  weighted GMRES solve per form, all on a seeded perturbed simple-wave state;
+* cli_*.npz    -- the reference euler2d command line on the configurations
+  its own tests and the headline 16x16 Q3 workload use: final coefficients
+  per form and the per-update _iterations.csv columns.
+
+Usage:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import csv
+import ctypes as C
+import json
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+REF = ROOT / "oracle" / "_ref"
+DP = C.POINTER(C.c_double)
+IP = C.POINTER(C.c_int)
+
+
+def ptr(a):
+    return a.ctypes.data_as(DP)
+
+
+def load_ref():
+    lib = C.CDLL(str(REF / "libeuler_ref.so"))
+    lib.ref_problem_new.restype = C.c_void_p
+    lib.ref_problem_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, C.c_double]
+    lib.ref_last_error.restype = C.c_char_p
+    lib.ref_cell_norm.restype = C.c_double
+    for name in ["ref_problem_free", "ref_sizes", "ref_geometry", "ref_tables", "ref_initial",
+                 "ref_freeze", "ref_set_old", "ref_set_dt", "ref_residual", "ref_cell_norm",
+                 "ref_admissible", "ref_dg_apply", "ref_dg_jacobi_blocks", "ref_hdg_condense",
+                 "ref_schur_apply", "ref_schur_jacobi_blocks", "ref_recover", "ref_linear_solve"]:
+        getattr(lib, name).argtypes = None
+    lib.ref_problem_free.argtypes = [C.c_void_p]
+    lib.ref_sizes.argtypes = [C.c_void_p, IP]
+    lib.ref_geometry.argtypes = [C.c_void_p, DP]
+    lib.ref_tables.argtypes = [C.c_void_p, DP, DP, DP, DP, DP, DP, DP, IP]
+    lib.ref_initial.argtypes = [C.c_void_p, DP]
+    lib.ref_freeze.argtypes = [C.c_void_p, DP, C.c_double, C.c_int, DP, DP, DP]
+    lib.ref_set_old.argtypes = [C.c_void_p, DP]
+    lib.ref_set_dt.argtypes = [C.c_void_p, C.c_double]
+    lib.ref_residual.argtypes = [C.c_void_p, DP, DP]
+    lib.ref_cell_norm.argtypes = [C.c_void_p, DP]
+    lib.ref_admissible.argtypes = [C.c_void_p, DP]
+    lib.ref_dg_apply.argtypes = [C.c_void_p, DP, DP, DP]
+    lib.ref_dg_jacobi_blocks.argtypes = [C.c_void_p, DP, DP]
+    lib.ref_hdg_condense.argtypes = [C.c_void_p, DP, DP, DP, DP, DP, DP]
+    lib.ref_schur_apply.argtypes = [C.c_void_p, DP, DP]
+    lib.ref_schur_jacobi_blocks.argtypes = [C.c_void_p, DP]
+    lib.ref_recover.argtypes = [C.c_void_p, DP, DP]
+    lib.ref_linear_solve.argtypes = [C.c_void_p, C.c_int, DP, DP, DP, DP, IP, DP]
+    return lib
+
+
+def check(lib, rc):
+    if rc:
+        raise RuntimeError(lib.ref_last_error().decode())
+
+
+# (nx, ny, k, alpha_deg, store_dense): small meshes cover every degree;
+# 16x16 Q3 is the headline workload's mesh.
+UNIT_CASES = [
+    (3, 2, 0, 45.0, True), (3, 2, 1, 45.0, True), (4, 3, 2, 30.0, True), (3, 3, 3, 60.0, True),
+    (16, 16, 3, 45.0, False), (4, 4, 4, 30.0, True), (3, 2, 5, 45.0, False), (2, 3, 6, 52.0, False),
+    (2, 2, 7, 41.0, False), (2, 2, 8, 37.0, False),
+]
+
+
+def make_unit(lib, nx, ny, k, alpha, dense, rng):
+    h = lib.ref_problem_new(nx, ny, k, alpha, 1.1, 0, 0, 20, 1500, 1e-12)
+    if not h:
+        raise RuntimeError(lib.ref_last_error().decode())
+    try:
+        sz = np.zeros(7, np.int32)
+        lib.ref_sizes(h, sz.ctypes.data_as(IP))
+        n, p, m, t, nf, nu, nl = map(int, sz)
+        q = k + 1
+        geo = np.zeros(5)
+        lib.ref_geometry(h, ptr(geo))
+        w, ew, im, ms = np.zeros(p), np.zeros(q), np.zeros(p), np.zeros(p)
+        tdx, tdy, fv = np.zeros(q * q), np.zeros(q * q), np.zeros(4 * q * p)
+        tn = np.zeros(p, np.int32)
+        lib.ref_tables(h, ptr(w), ptr(ew), ptr(im), ptr(ms), ptr(tdx), ptr(tdy), ptr(fv),
+                       tn.ctypes.data_as(IP))
+        u0 = np.zeros(nu)
+        check(lib, lib.ref_initial(h, ptr(u0)))
+        # Coarse meshes can make the projected wave inadmissible at face
+        # points; blend toward the mean state as the reference's --verify does
+        # (src/verification.cpp:26-30) until the state is admissible, then
+        # apply a seeded node-wise perturbation.
+        background = np.tile(u0.reshape(-1, 4).mean(axis=0), nu // 4)
+        node_scale = np.repeat(1.0 + 0.01 * np.sin(0.37 * np.arange(nu // 4) + 0.3), 4)
+        noise = 1e-5 * rng.standard_normal(nu)
+        for blend in (1.0, 0.5, 0.2, 0.05):
+            base = blend * u0 + (1 - blend) * background
+            u = base * node_scale + noise * np.abs(base)
+            if lib.ref_admissible(h, ptr(u)):
+                break
+        else:
+            raise RuntimeError("no admissible perturbed state")
+        dt = 0.05 * min(geo[2], geo[3])
+        a, b, rate = np.zeros(nf * q), np.zeros(nf * q), np.zeros(1)
+        check(lib, lib.ref_freeze(h, ptr(u), dt, 1, ptr(a), ptr(b), ptr(rate)))
+        old = u0.copy()
+        check(lib, lib.ref_set_old(h, ptr(old)))
+        lib.ref_set_dt(h, dt)
+        r = np.zeros(nu)
+        check(lib, lib.ref_residual(h, ptr(u), ptr(r)))
+        x = rng.standard_normal(nu)
+        jx = np.zeros(nu)
+        check(lib, lib.ref_dg_apply(h, ptr(u), ptr(x), ptr(jx)))
+        out = dict(nx=nx, ny=ny, k=k, alpha=alpha, dt=dt, blend=blend, geometry=geo, w=w, ew=ew, inv_mass=im,
+                   mass=ms, tensor_dx=tdx, tensor_dy=tdy, fv=fv, tensor_node=tn, u0=u0, u=u, old=old,
+                   a=a, b=b, rate=rate, r=r, x=x, jx=jx,
+                   r_norm=np.array([lib.ref_cell_norm(h, ptr(r))]))
+        if dense:
+            blocks = np.zeros(n * m * m)
+            check(lib, lib.ref_dg_jacobi_blocks(h, ptr(u), ptr(blocks)))
+            out["dg_blocks"] = blocks
+        rhs, X, y, D = np.zeros(nl), np.zeros(n * m * 4 * t), np.zeros(nu), np.zeros(nl)
+        check(lib, lib.ref_hdg_condense(h, ptr(u), ptr(r), ptr(rhs), ptr(X), ptr(y), ptr(D)))
+        out.update(rhs=rhs, y_hdg=y, D=D)
+        if dense:
+            out["X"] = X
+            sblocks = np.zeros(nf * t * t)
+            check(lib, lib.ref_schur_jacobi_blocks(h, ptr(sblocks)))
+            out["schur_blocks"] = sblocks
+        v = rng.standard_normal(nl)
+        sv = np.zeros(nl)
+        check(lib, lib.ref_schur_apply(h, ptr(v), ptr(sv)))
+        lam = rng.standard_normal(nl)
+        du = np.zeros(nu)
+        check(lib, lib.ref_recover(h, ptr(lam), ptr(du)))
+        out.update(v=v, sv=sv, lam=lam, du=du)
+        for form, (rhs_f, N) in {0: (-r, nu), 1: (rhs, nl)}.items():
+            rr = np.ascontiguousarray(rhs_f)
+            xs, eq = np.zeros(N), np.zeros(N)
+            cnt, rel = np.zeros(1, np.int32), np.zeros(1)
+            check(lib, lib.ref_linear_solve(h, form, ptr(u), ptr(rr), ptr(xs), ptr(eq),
+                                            cnt.ctypes.data_as(IP), ptr(rel)))
+            tag = "dg" if form == 0 else "hdg"
+            out[f"solve_{tag}_x"] = xs
+            out[f"solve_{tag}_count"] = cnt
+            out[f"solve_{tag}_relres"] = rel
+        return out
+    finally:
+        lib.ref_problem_free(h)
+
+
+def ref_cli() -> Path:
+    v4 = REF / "euler2d_ref_v4"
+    try:
+        subprocess.run([str(v4), "--help"], capture_output=True, check=True)
+        return v4
+    except (OSError, subprocess.CalledProcessError):
+        return REF / "euler2d_ref_v3"
+
+
+# name -> argument list (the reference's code tests and the 16x16 Q3 workload)
+CLI_CASES = {
+    "c1_16x16_q3": ["--nx", "16", "--ny", "16", "--k", "3", "--alpha-deg", "45", "--cfl", "1",
+                    "--steps", "3", "--newton-steps", "3", "--form", "both", "--assembly", "partial",
+                    "--precond", "block-jacobi"],
+    "be1_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "45", "--cfl", "1",
+                   "--steps", "1", "--newton-steps", "1", "--integrator", "be", "--form", "both"],
+    "smoke_8x8_q1": ["--nx", "8", "--ny", "8", "--k", "1", "--cfl", ".1", "--steps", "1",
+                     "--form", "both", "--newton-tol", "1e-12", "--linear-tol", "1e-12"],
+    "be_converged_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--cfl", ".1", "--steps", "1",
+                            "--integrator", "be", "--form", "both", "--check-update",
+                            "--newton-tol", "1e-12", "--linear-tol", "1e-12"],
+}
+ITER_COLS = ["step", "stage", "newton", "time", "dt", "cfl", "residual_physical_rms", "damping",
+             "krylov_iterations", "linear_relative_residual", "dg_linear_relative_residual",
+             "update_check_relative"]
+SUMMARY_COLS = ["T", "actual_max_cfl", "mean_dt", "volume_dofs", "trace_dofs", "time_steps",
+                "newton_updates", "rho_L2", "rhou_L2", "rhov_L2", "energy_L2", "max_conservation_drift"]
+
+
+def ref_initial_state(lib, args: list[str]) -> np.ndarray:
+    def opt(flag, default):
+        return type(default)(args[args.index(flag) + 1]) if flag in args else default
+    nx, ny, k, alpha = opt("--nx", 100), opt("--ny", 100), opt("--k", 1), opt("--alpha-deg", 45.0)
+    h = lib.ref_problem_new(nx, ny, k, alpha, 1.1, 0, 0, 20, 1500, 1e-12)
+    try:
+        sz = np.zeros(7, np.int32)
+        lib.ref_sizes(h, sz.ctypes.data_as(IP))
+        u0 = np.zeros(int(sz[5]))
+        check(lib, lib.ref_initial(h, ptr(u0)))
+        return u0
+    finally:
+        lib.ref_problem_free(h)
+
+
+def make_cli(exe: Path, name: str, args: list[str]) -> dict:
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = Path(tmp) / "run"
+        proc = subprocess.run([str(exe), *args, "--output", str(prefix)], capture_output=True, text=True)
+        if proc.returncode:
+            raise RuntimeError(f"{name}: {proc.stderr}")
+        out = {"args": np.array(json.dumps(args))}
+        for form in ("dg", "hdg"):
+            coeff = np.loadtxt(f"{prefix}_{form}_coefficients.csv", delimiter=",", skiprows=1)
+            out[f"{form}_u"] = coeff[:, 2:].reshape(-1)
+            with open(f"{prefix}_{form}_iterations.csv", newline="") as fh:
+                rows = list(csv.DictReader(fh))
+            out[f"{form}_iterations"] = np.array([[float(r[c]) for c in ITER_COLS] for r in rows])
+            with open(f"{prefix}_{form}_summary.csv", newline="") as fh:
+                row = next(csv.DictReader(fh))
+            out[f"{form}_summary"] = np.array([float(row[c]) for c in SUMMARY_COLS])
+        with open(f"{prefix}_comparison.csv", newline="") as fh:
+            row = next(csv.DictReader(fh))
+        out["comparison"] = np.array([float(v) for v in row.values()])
+        return out
+
+
+def main():
+    if not (REF / "libeuler_ref.so").exists():
+        sys.exit("oracle/_ref is not built: run `make -C oracle` where the reference is available")
+    lib = load_ref()
+    rng = np.random.default_rng(20261203)
+    for nx, ny, k, alpha, dense in UNIT_CASES:
+        data = make_unit(lib, nx, ny, k, alpha, dense, rng)
+        np.savez_compressed(HERE / f"units_{nx}x{ny}_k{k}.npz", **data)
+        print("unit", nx, ny, k)
+    exe = ref_cli()
+    for name, args in CLI_CASES.items():
+        data = make_cli(exe, name, args)
+        data["u0"] = ref_initial_state(lib, args)
+        np.savez_compressed(HERE / f"cli_{name}.npz", **data)
+        print("cli", name)
+    meta = {"iteration_columns": ITER_COLS, "summary_columns": SUMMARY_COLS,
+            "unit_cases": UNIT_CASES, "cli_cases": CLI_CASES}
+    (HERE / "manifest.json").write_text(json.dumps(meta, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,86 @@
+"""CPU-side checks of the C-ABI boundary: the library loads without a GPU,
+exports every function include/euler2d_cuda.h declares, builds the
+reference's host tables bit for bit, and the euler2d command line validates
+options exactly like the reference (src/options.cpp) before touching CUDA."""
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, unit_files
+from mfem_euler2d_cpp_b200 import capi
+
+CLI = ROOT / "mfem_euler2d_cpp_b200" / "bin" / "euler2d"
+
+
+def test_library_exports_every_declared_symbol():
+    lib = capi.load()
+    names = capi.declared_symbols()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert missing == []
+
+
+def test_status_strings_match_reference_messages():
+    lib = capi.load()
+    assert lib.eg_status_string(12) == b"GMRES iteration limit reached"
+    assert lib.eg_status_string(16) == b"Newton line search failed"
+    assert lib.eg_status_string(7) == b"Singular streaming HDG cell factor"
+    assert lib.eg_status_string(14) == b"Recovered DG residual criterion failed after Schur refinement"
+
+
+@pytest.mark.parametrize("path", unit_files(), ids=lambda p: p.stem)
+def test_host_tables_match_reference(path):
+    f = np.load(path)
+    nx, ny, k, alpha = int(f["nx"]), int(f["ny"]), int(f["k"]), float(f["alpha"])
+    d = capi.simple_wave_desc(nx, ny, k, alpha)
+    q, p = k + 1, (k + 1) ** 2
+    lx, ly, hx, hy, area = f["geometry"]
+    assert (d.lx, d.ly, d.hx, d.hy, d.area) == (lx, ly, hx, hy, area)
+    np.testing.assert_array_equal(np.array(d.w[:p]), f["w"])
+    np.testing.assert_array_equal(np.array(d.ew[:q]), f["ew"])
+    np.testing.assert_array_equal(np.array(d.inv_mass[:p]), f["inv_mass"])
+    np.testing.assert_array_equal(np.array(d.mass[:p]), f["mass"])
+    np.testing.assert_array_equal(np.array(d.tensor_dx[:q * q]), f["tensor_dx"])
+    np.testing.assert_array_equal(np.array(d.tensor_dy[:q * q]), f["tensor_dy"])
+    np.testing.assert_array_equal(np.array(d.tensor_node[:p]), f["tensor_node"])
+    fv = f["fv"].reshape(4, q, p)
+    fb = np.array(d.face_basis[:4 * q * q]).reshape(4, q, q)
+    for s in range(4):
+        for j in range(q):
+            for l in range(q):
+                node = j * q + l if s < 2 else l * q + j
+                assert fb[s, j, l] == fv[s, j, node]
+            # every other node of the reference table is zero on this face point
+            on_line = {j * q + l if s < 2 else l * q + j for l in range(q)}
+            assert all(fv[s, j, i] == 0 for i in range(p) if i not in on_line)
+
+
+def _cli(*args):
+    return subprocess.run([str(CLI), *args], capture_output=True, text=True, timeout=60)
+
+
+@pytest.mark.parametrize("args,message", [
+    (["--k", "9"], "Invalid mesh, degree, time or safety"),
+    (["--nx", "1"], "Invalid mesh, degree, time or safety"),
+    (["--form", "cg"], "Invalid form"),
+    (["--integrator", "rk4"], "Invalid time integrator"),
+    (["--precond", "amg"], "Invalid preconditioner"),
+    (["--alpha-deg", "90"], "Require 0 < alpha-deg < 90"),
+    (["--cfl", "-1"], "--cfl must be positive"),
+    (["--bogus"], "Unknown option: --bogus"),
+    (["--nx"], "Missing option value"),
+    (["--volume-order", "5"], "Volume rule must be (k+1)^2 GL points (order 2k+1)"),
+    (["--device", "cpu"], "This executable is the --device cuda path"),
+])
+def test_cli_rejects_invalid_options(args, message):
+    proc = _cli(*args)
+    assert proc.returncode == 1
+    assert proc.stderr.startswith("ERROR: ")
+    assert message in proc.stderr
+
+
+def test_cli_help():
+    proc = _cli("--help")
+    assert proc.returncode == 0
+    assert "--form dg|hdg|both" in proc.stdout
