@@ -1,0 +1,508 @@
+#!/usr/bin/env python3
+"""Benchmark: mean seconds per accepted Newton update on one B200.
+
+Workload (default): 128x128 periodic Q4 simple wave, gamma=3, alpha=30 deg,
+condensed HDG with partial assembly and block-Jacobi right-preconditioned
+GMRES, SSP-DIRK3 at CFL 1, 3 Newton updates per stage. A "step" is one
+accepted Newton update of that schedule (residual -> condensation -> Schur
+GMRES -> recovery -> validation -> line search), advanced through the C-ABI
+stepper. Inputs are synthetic: the seeded, deterministic simple-wave initial
+condition (no dataset exists for this problem).
+
+Arms
+  (default)        the CUDA engine (mfem_euler2d_cpp_b200/lib/libeuler2d_cuda.so)
+  --impl reference the reference's own CPU code (oracle/_ref, the unmodified
+                   reference sources built against the MFEM-subset shim), one
+                   thread on the host, bounded sample of the same workload.
+
+Multi-GPU: the update does not shard across GPUs in this build; N ranks run N
+independent replicas (weak scaling, no data-path collective). value is the
+whole-job time per update: max over ranks of the timed region / (N * K).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import json
+import math
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "c2": dict(nx=128, ny=128, k=4, alpha=30.0, form="hdg", precond="block-jacobi", cfl=1.0, steps=5,
+               newton_steps=3,
+               label="128x128 periodic Q4 simple wave (gamma=3, alpha=30deg), HDG condensed, partial "
+                     "assembly, block-Jacobi GMRES, SSP-DIRK3 CFL 1, 5 steps x 3 Newton updates"),
+    "c1": dict(nx=16, ny=16, k=3, alpha=45.0, form="hdg", precond="block-jacobi", cfl=1.0, steps=3,
+               newton_steps=3,
+               label="16x16 periodic Q3 simple wave (gamma=3, alpha=45deg), HDG condensed, partial "
+                     "assembly, block-Jacobi GMRES, SSP-DIRK3 CFL 1, 3 steps x 3 Newton updates"),
+    "c3": dict(nx=256, ny=256, k=3, alpha=45.0, form="hdg", precond="block-jacobi", cfl=1.0, steps=5,
+               newton_steps=3,
+               label="256x256 periodic Q3 simple wave (gamma=3, alpha=45deg), HDG condensed, FP64"),
+}
+METRIC = "mean s per accepted Newton update"
+K_NAMES = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "recover",
+           "recovered_residual", "schur_jacobi", "pc_apply", "krylov", "freeze", "admissible", "vector"]
+
+
+def sizes(w):
+    q = w["k"] + 1
+    p, n = q * q, w["nx"] * w["ny"]
+    m, t = 4 * p, 4 * q
+    return dict(q=q, p=p, n=n, m=m, t=t, nf=2 * n, nu=n * m, nl=2 * n * t)
+
+
+def algorithmic(w):
+    """Per-launch algorithmic bytes / flops of the hot kernels (FP64)."""
+    s = sizes(w)
+    n, m, t, q, p, nu, nl, nf = s["n"], s["m"], s["t"], s["q"], s["p"], s["nu"], s["nl"], s["nf"]
+    return {
+        "schur_apply": ("hbm", 8.0 * (n * m * 4 * t + 64 * n * q + 3 * nl)),
+        "recover": ("hbm", 8.0 * (n * m * 4 * t + n * m + nl + nu)),
+        "dg_apply": ("hbm", 8.0 * (2 * nu + 32 * n * p + 32 * nf * q)),
+        "residual": ("hbm", 8.0 * (3 * nu + 6 * nf * q)),
+        "pc_apply": ("hbm", 8.0 * (nf * t * t + 2 * nl) if w["form"] == "hdg" else 8.0 * (n * m * m + 2 * nu)),
+        "condense": ("fp64", n * (2.0 / 3.0 * m ** 3 + 2.0 * m * m * (4 * t + 1))),
+        "dg_jacobi": ("fp64", n * (2.0 / 3.0 * m ** 3)),
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, out: Path, gpu_index: int):
+        self.out, self.gpu_index, self.proc = out, gpu_index, None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.fh = open(self.out, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                      "-i", str(self.gpu_index), "-lms", "200"], stdout=self.fh,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in self.out.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1].split()[0]), smax=float(parts[2].split()[0]),
+                                 power=float(parts[3].split()[0]) if parts[3][0].isdigit() else 0.0,
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], pcap=parts[8]))
+            except (ValueError, IndexError):
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        reasons = []
+        for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                          ("swt", "sw_thermal_slowdown"), ("pcap", "sw_power_cap")):
+            if any(r[key].lower().startswith("active") for r in rows):
+                reasons.append(name)
+        return {"sm_mhz": float(np.median([r["sm"] for r in rows])),
+                "sm_max_mhz": max(r["smax"] for r in rows), "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(r["power"] for r in rows)}
+
+
+# ------------------------------------------------------------ CPU reference
+def ref_binary():
+    ref = ROOT / "oracle" / "_ref"
+    for name in ("euler2d_ref_v4", "euler2d_ref_v3"):
+        exe = ref / name
+        if exe.exists():
+            try:
+                subprocess.run([str(exe), "--help"], capture_output=True, check=True, timeout=30)
+                return exe
+            except (OSError, subprocess.CalledProcessError, subprocess.TimeoutExpired):
+                continue
+    return None
+
+
+def run_reference_updates(w, newton_steps: int, timeout: float = 900.0):
+    """Run the reference CLI on the first SSP-DIRK3 step of the workload with
+    `newton_steps` updates per stage, single-threaded on one core. Returns the
+    per-update iteration_s list (the reference's own update timer)."""
+    exe = ref_binary()
+    if exe is None:
+        return None, "oracle/_ref binaries not built"
+    env = dict(os.environ)
+    for name in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        env[name] = "1"
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = Path(tmp) / "ref"
+        cmd = [str(exe), "--nx", str(w["nx"]), "--ny", str(w["ny"]), "--k", str(w["k"]),
+               "--alpha-deg", str(w["alpha"]), "--cfl", str(w["cfl"]), "--steps", "1",
+               "--newton-steps", str(newton_steps), "--form", w["form"], "--precond", w["precond"],
+               "--assembly", "partial", "--no-save-solution", "--output", str(prefix)]
+        if shutil.which("taskset"):
+            cmd = ["taskset", "-c", "0"] + cmd
+        proc = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
+        if proc.returncode:
+            return None, proc.stderr.strip()[-300:]
+        with open(f"{prefix}_{w['form']}_iterations.csv", newline="") as fh:
+            times = [float(r["iteration_s"]) for r in csv.DictReader(fh)]
+    return times, exe.name
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------- helpers
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_context(w, form, device=0):
+    from mfem_euler2d_cpp_b200 import capi
+
+    lib = capi.load()
+    if lib.eg_set_device(device) != capi.OK:
+        raise RuntimeError("eg_set_device failed")
+    d = capi.simple_wave_desc(w["nx"], w["ny"], w["k"], w["alpha"])
+    o = capi.default_opts(form=capi.FORM_HDG if form == "hdg" else capi.FORM_DG,
+                          precond=capi.PC_JACOBI if w["precond"] == "block-jacobi" else capi.PC_ILU0)
+    return capi.Context(d, o)
+
+
+def make_stepper(ctx, w, total_updates, form):
+    from mfem_euler2d_cpp_b200 import capi
+
+    per_step = 4 * w["newton_steps"]
+    steps = max(w["steps"], math.ceil(total_updates / per_step) + 1)
+    ro, keep = capi.run_options(integrator="ssp-dirk3", steps=steps, newton_steps=w["newton_steps"],
+                                cfl=w["cfl"], form_name=form, precond_name=w["precond"])
+    return capi.Stepper(ctx, ro, keep)
+
+
+def timed_updates(ctx, stepper, K, world, events_stream, host_io=None):
+    """Time exactly K accepted updates with CUDA events on the engine stream.
+    host_io=(pinned numpy in, pinned numpy out) adds the H2D upload of the
+    state and the D2H read of the result to every step."""
+    import torch
+
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    device_ms = 0.0
+    barrier(world)
+    torch.cuda.synchronize()
+    start.record(events_stream)
+    for _ in range(K):
+        if host_io is not None:
+            ctx.upload_ptr("U", host_io[0].ctypes.data)
+        st = stepper.next()
+        if st is None:
+            raise RuntimeError("schedule exhausted")
+        device_ms += st.device_ms
+        if host_io is not None:
+            ctx.download_ptr("U", host_io[1].ctypes.data)
+    end.record(events_stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    return start.elapsed_time(end), device_ms
+
+
+def fp64_gemm_peak():
+    """Measured FP64 GEMM rate (torch/cuBLAS DGEMM, 4096^3, best of 5)."""
+    import torch
+
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ------------------------------------------------------------------- arms
+def run_ours(args, world, rank, local):
+    import torch
+
+    from mfem_euler2d_cpp_b200 import capi
+
+    w = dict(WORKLOADS[args.workload])
+    K, W = args.steps, args.warmup
+    torch.cuda.set_device(local)
+    ctx = make_context(w, w["form"], local)
+    stepper = make_stepper(ctx, w, W + 2 * K, w["form"])
+    ext = torch.cuda.ExternalStream(ctx.stream_ptr())
+    for _ in range(W):
+        if stepper.next() is None:
+            raise RuntimeError("schedule exhausted during warm-up")
+    ctx.lib.eg_profile_reset(ctx.h)
+    ctx.lib.eg_profile_enable(ctx.h, 1)
+    launches0 = ctx.lib.eg_launch_count(ctx.h)
+    phys = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            phys = int(vis.split(",")[local])
+        except ValueError:
+            phys = local
+    sampler = ClockSampler(Path(tempfile.gettempdir()) / f"eg_clocks_{rank}.csv", phys)
+    sampler.start()
+    time.sleep(0.3)
+    elapsed_ms, dev_ms = timed_updates(ctx, stepper, K, world, ext)
+    clocks = sampler.stop()
+    launches = ctx.lib.eg_launch_count(ctx.h) - launches0
+    prof = {}
+    for i, name in enumerate(K_NAMES):
+        import ctypes as C
+
+        ms, cnt = C.c_double(), C.c_longlong()
+        ctx.lib.eg_profile_query(ctx.h, i, C.byref(ms), C.byref(cnt))
+        prof[name] = (ms.value, cnt.value)
+    ctx.lib.eg_profile_enable(ctx.h, 0)
+    # end to end: the state crosses the host boundary every update
+    nu = ctx.nu
+    pin_in = torch.empty(nu, dtype=torch.float64, pin_memory=True).numpy()
+    pin_out = torch.empty(nu, dtype=torch.float64, pin_memory=True).numpy()
+    pin_in[:] = ctx.download("U")
+    e2e_ms, _ = timed_updates(ctx, stepper, K, world, ext, host_io=(pin_in, pin_out))
+    elapsed_ms = max_over_ranks(world, elapsed_ms)
+    e2e_ms = max_over_ranks(world, e2e_ms)
+    dev_ms = max_over_ranks(world, dev_ms)
+    dev_bytes = ctx.device_bytes()
+    ctx_sizes = sizes(w)
+    stepper.close()
+    ctx.close()
+    torch.cuda.synchronize()
+
+    # DG form of the same workload (secondary line)
+    dg = None
+    if not args.no_dg:
+        ctxd = make_context(w, "dg", local)
+        std = make_stepper(ctxd, w, W + K, "dg")
+        extd = torch.cuda.ExternalStream(ctxd.stream_ptr())
+        for _ in range(W):
+            std.next()
+        dg_ms, dg_dev = timed_updates(ctxd, std, K, world, extd)
+        dg_ms = max_over_ranks(world, dg_ms)
+        dg = {"value": dg_ms * 1e-3 / (K * world), "unit": "s", "ms_per_step": dg_ms / K,
+              "mean_newton_device_s": dg_dev * 1e-3 / K, "form": "dg"}
+        std.close()
+        ctxd.close()
+
+    if rank != 0:
+        return None
+    peaks, peak_src = measured_peaks()
+    alg = algorithmic(w)
+    dominant = max(prof, key=lambda k: prof[k][0])
+    roofline = None
+    fp64_peak = None
+    dom_ms, dom_launch = prof[dominant]
+    ops_per = {"schur_apply": 2, "condense": 2}.get(dominant, 1)
+    nops = max(1, dom_launch // ops_per)
+    if dominant in alg:
+        kind, units = alg[dominant]
+        avg_s = dom_ms * 1e-3 / nops
+        if kind == "hbm":
+            achieved = units / avg_s / 1e9
+            peak = peaks["hbm_gbs"]
+            roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                        "algorithmic_bytes_per_launch": units, "avg_launch_ms": avg_s * 1e3,
+                        "launches": nops, "peak_source": f"{peak_src} hbm_gbs"}
+        else:
+            fp64_peak = fp64_gemm_peak()
+            achieved = units / avg_s / 1e12
+            roofline = {"kernel": dominant, "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
+                        "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                        "algorithmic_flops_per_launch": units, "avg_launch_ms": avg_s * 1e3,
+                        "launches": nops,
+                        "peak_source": "measured FP64 DGEMM (torch.matmul float64 4096^3) on this GPU"}
+    # second roofline line for the HBM-bound Schur apply (the matrix-free hot loop)
+    hbm_lines = {}
+    for name in ("schur_apply", "recover", "pc_apply", "residual", "dg_apply"):
+        ms, cnt = prof[name]
+        per = 2 if name == "schur_apply" else 1
+        n_op = cnt // per
+        if n_op and name in alg:
+            avg_s = ms * 1e-3 / n_op
+            ach = alg[name][1] / avg_s / 1e9
+            hbm_lines[name] = {"achieved_gbs": ach, "frac": ach / peaks["hbm_gbs"], "avg_launch_ms": avg_s * 1e3,
+                               "launches": n_op}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        times, src = run_reference_updates(w, 1)
+        if times:
+            cpu = {"value": float(np.mean(times)), "unit": "s", "cores": 1, "kind": "reference",
+                   "sample": f"first SSP-DIRK3 step of the same workload, 1 Newton update per stage "
+                             f"({len(times)} updates), reference's own per-update timer; {src} on "
+                             f"'{cpu_model()}', one thread pinned with taskset",
+                   "per_update_s": times}
+        else:
+            cpu = {"value": None, "unit": "s", "cores": 1, "kind": "reference", "sample": f"unavailable: {src}"}
+    value = elapsed_ms * 1e-3 / (K * world)
+    line = {
+        "metric": f"{METRIC} (HDG, {w['nx']}x{w['ny']} Q{w['k']}, block-Jacobi)",
+        "value": value, "unit": "s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": elapsed_ms / K, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: deterministic simple-wave initial condition (gamma=3) projected on the mesh",
+        "config": {"workload": w["label"], "nx": w["nx"], "ny": w["ny"], "k": w["k"], "alpha_deg": w["alpha"],
+                   "form": w["form"], "precond": w["precond"], "integrator": "ssp-dirk3", "cfl": w["cfl"],
+                   "newton_steps_per_stage": w["newton_steps"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (condensed responses X are %.2f GB per update)"
+                         % (8 * ctx_sizes["n"] * ctx_sizes["m"] * 4 * ctx_sizes["t"] / 1e9),
+                   "body_dofs": ctx_sizes["nu"], "trace_dofs": ctx_sizes["nl"],
+                   "device_bytes": dev_bytes},
+        "updates_per_s": K * world / (elapsed_ms * 1e-3),
+        "mean_newton_device_s": dev_ms * 1e-3 / K,
+        "e2e": {"value": e2e_ms * 1e-3 / (K * world), "unit": "s", "h2d_bytes_per_step": 8 * ctx_sizes["nu"],
+                "d2h_bytes_per_step": 8 * ctx_sizes["nu"],
+                "path": "eg_upload(U) + eg_stepper_next + eg_download(U) per update, pinned host buffers"},
+        "roofline": roofline,
+        "hbm_kernels": hbm_lines,
+        "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]},
+        "kernel_launches": {k: v[1] for k, v in prof.items() if v[1]},
+        "gpu_launches": int(launches),
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "dg": dg,
+    }
+    return line
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return None
+    w = dict(WORKLOADS[args.workload])
+    K, W = args.steps, args.warmup
+    # bounded sample: at most 12 reference updates (about 3 minutes at 128^2 Q4)
+    total = min(W + K, args.ref_max_updates)
+    n_per_stage = max(1, math.ceil(total / 4))
+    times, src = run_reference_updates(w, n_per_stage, timeout=1800)
+    if not times:
+        return {"impl": "reference", "unavailable": f"reference CPU build could not run: {src}"}
+    warm = min(W, len(times) - 1)
+    timed = times[warm:warm + K]
+    value = float(np.mean(timed))
+    return {
+        "impl": "reference",
+        "metric": f"{METRIC} (HDG, {w['nx']}x{w['ny']} Q{w['k']}, block-Jacobi)",
+        "value": value, "unit": "s", "n_gpus": world, "steps": len(timed), "warmup": warm,
+        "requested_steps": K, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: deterministic simple-wave initial condition (gamma=3) projected on the mesh",
+        "config": {"workload": w["label"], "nx": w["nx"], "ny": w["ny"], "k": w["k"],
+                   "form": w["form"], "precond": w["precond"], "parallelism": "single-threaded CPU"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "reference",
+                         "sample": f"first SSP-DIRK3 step, {n_per_stage} Newton updates per stage "
+                                   f"({len(times)} updates, first {warm} untimed); unmodified reference "
+                                   f"sources built against the MFEM-subset shim ({src}) on '{cpu_model()}'"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "per_update_s": timed,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--no-dg", action="store_true", help="skip the secondary DG-form measurement")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-max-updates", type=int, default=12)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference_arm(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        line = run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -150,6 +150,10 @@ typedef struct eg_ctx eg_ctx;
 int eg_desc_simple_wave(eg_desc *d, int nx, int ny, int k, double alpha_deg, double gamma,
                         double safety);
 void eg_opts_default(eg_opts *o);
+/* Select the CUDA device for contexts created later on the calling thread
+ * (the library links its own CUDA runtime, so callers that chose a device
+ * through another runtime must select it here as well). */
+int eg_set_device(int device);
 
 /* Replaces: Problem construction + PrepareHybrid + LinearSolver construction
  * (src/problem.cpp:32, src/condensation.cpp:47, src/linear.cpp:159). */
@@ -268,6 +272,23 @@ typedef struct eg_stepper eg_stepper;
 int eg_stepper_create(eg_ctx *ctx, const eg_run_opts *ro, eg_stepper **out);
 int eg_stepper_next(eg_stepper *s, eg_update_stats *st);
 void eg_stepper_destroy(eg_stepper *s);
+
+/* ------------------------------------------------------------ profiling */
+/* Kernel classes timed with CUDA events on the context stream when
+ * profiling is on (eg_profile_enable). */
+enum eg_kernel_class {
+  EG_K_RESIDUAL = 0, EG_K_DG_APPLY = 1, EG_K_DG_JACOBI = 2, EG_K_CONDENSE = 3,
+  EG_K_SCHUR_APPLY = 4, EG_K_RECOVER = 5, EG_K_RECOVERED_RESIDUAL = 6, EG_K_SCHUR_JACOBI = 7,
+  EG_K_PC_APPLY = 8, EG_K_KRYLOV = 9, EG_K_FREEZE = 10, EG_K_ADMISSIBLE = 11, EG_K_VECTOR = 12,
+  EG_K_COUNT = 13
+};
+int eg_profile_enable(eg_ctx *ctx, int on);
+int eg_profile_reset(eg_ctx *ctx);
+/* Accumulated device milliseconds and launch count of one kernel class since
+ * the last reset (synchronises the context stream). */
+int eg_profile_query(eg_ctx *ctx, int kernel_class, double *ms, long long *launches);
+/* Total kernels launched on the context since creation. */
+long long eg_launch_count(const eg_ctx *ctx);
 
 #ifdef __cplusplus
 }

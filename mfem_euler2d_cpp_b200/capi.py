@@ -119,6 +119,11 @@ def load() -> C.CDLL:
         "eg_desc_simple_wave": (C.c_int, [C.POINTER(Desc), C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_double, C.c_double]),
         "eg_opts_default": (None, [C.POINTER(Opts)]),
+        "eg_set_device": (C.c_int, [C.c_int]),
+        "eg_profile_enable": (C.c_int, [vp, C.c_int]),
+        "eg_profile_reset": (C.c_int, [vp]),
+        "eg_profile_query": (C.c_int, [vp, C.c_int, _DP, C.POINTER(C.c_longlong)]),
+        "eg_launch_count": (C.c_longlong, [vp]),
         "eg_create": (C.c_int, [C.POINTER(Desc), C.POINTER(Opts), C.POINTER(vp)]),
         "eg_destroy": (None, [vp]),
         "eg_last_error": (C.c_char_p, [vp]),
@@ -316,6 +321,13 @@ class Context:
         st = UpdateStats()
         self._check(self.lib.eg_newton_update(self.h, residual_norm, old_norm, C.byref(st)))
         return st
+
+    def upload_ptr(self, slot: str, ptr: int):
+        """Upload from a raw host or device address (no intermediate copy)."""
+        self._check(self.lib.eg_upload(self.h, SLOT[slot], C.cast(C.c_void_p(ptr), _DP)))
+
+    def download_ptr(self, slot: str, ptr: int):
+        self._check(self.lib.eg_download(self.h, SLOT[slot], C.cast(C.c_void_p(ptr), _DP)))
 
     def stream_ptr(self) -> int:
         return int(self.lib.eg_stream(self.h) or 0)

@@ -65,6 +65,50 @@ void *Ctx::alloc(size_t nbytes) {
 
 void Ctx::sync() { EG_CUDA(cudaStreamSynchronize(stream)); }
 
+static cudaEvent_t take_event(Ctx &c) {
+  if (!c.prof.pool.empty()) {
+    cudaEvent_t e = c.prof.pool.back();
+    c.prof.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  EG_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+ProfScope::ProfScope(Ctx &ctx, int kernel_class, long long nlaunch)
+    : c(ctx), id(kernel_class), launches(nlaunch) {
+  c.launches += nlaunch;
+  if (c.prof.on) {
+    a = take_event(c);
+    b = take_event(c);
+    cudaEventRecord(a, c.stream);
+  }
+}
+ProfScope::~ProfScope() {
+  if (a) {
+    cudaEventRecord(b, c.stream);
+    c.prof.pending.push_back({id, launches, a, b});
+    if (c.prof.pending.size() > 4096) {
+      cudaStreamSynchronize(c.stream);
+      c.prof_resolve();
+    }
+  }
+}
+
+void Ctx::prof_resolve() {
+  for (auto &r : prof.pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      prof.ms[r.id] += ms;
+      prof.count[r.id] += r.launches;
+    }
+    prof.pool.push_back(r.a);
+    prof.pool.push_back(r.b);
+  }
+  prof.pending.clear();
+}
+
 void Ctx::check_device_error() {
   EG_CUDA(cudaMemcpyAsync(herr, derr, sizeof(int), cudaMemcpyDeviceToHost, stream));
   sync();
@@ -371,6 +415,16 @@ int eg_desc_simple_wave(eg_desc *d, int nx, int ny, int k, double alpha_deg, dou
   return EG_OK;
 }
 
+int eg_set_device(int device) {
+  const cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    g_create_error = cudaGetErrorString(e);
+    return EG_ERR_CUDA;
+  }
+  return EG_OK;
+}
+
 void eg_opts_default(eg_opts *o) {
   o->form = EG_FORM_HDG;
   o->precond = EG_PC_BLOCK_JACOBI;
@@ -481,6 +535,11 @@ void eg_destroy(eg_ctx *ctx) {
   if (!ctx) return;
   Ctx &c = ctx->c;
   if (c.stream) cudaStreamSynchronize(c.stream);
+  for (auto &r : c.prof.pending) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : c.prof.pool) cudaEventDestroy(e);
   for (void *p : c.allocations) cudaFree(p);
   if (c.hctl) cudaFreeHost(c.hctl);
   if (c.hscal) cudaFreeHost(c.hscal);
@@ -762,6 +821,33 @@ int eg_errors(eg_ctx *ctx, double time, double out[4]) {
     eg::host::errors(c.desc, u.data(), time, out);
   });
 }
+
+int eg_profile_enable(eg_ctx *ctx, int on) {
+  if (!ctx) return EG_ERR_INVALID;
+  ctx->c.prof.on = on != 0;
+  return EG_OK;
+}
+int eg_profile_reset(eg_ctx *ctx) {
+  if (!ctx) return EG_ERR_INVALID;
+  return guard(ctx, [&] {
+    ctx->c.sync();
+    ctx->c.prof_resolve();
+    for (int i = 0; i < EG_K_COUNT; ++i) {
+      ctx->c.prof.ms[i] = 0.;
+      ctx->c.prof.count[i] = 0;
+    }
+  });
+}
+int eg_profile_query(eg_ctx *ctx, int kernel_class, double *ms, long long *launches) {
+  if (!ctx || kernel_class < 0 || kernel_class >= EG_K_COUNT) return EG_ERR_INVALID;
+  return guard(ctx, [&] {
+    ctx->c.sync();
+    ctx->c.prof_resolve();
+    if (ms) *ms = ctx->c.prof.ms[kernel_class];
+    if (launches) *launches = ctx->c.prof.count[kernel_class];
+  });
+}
+long long eg_launch_count(const eg_ctx *ctx) { return ctx ? ctx->c.launches : 0; }
 
 int eg_differences(const eg_desc *d, const double *u, const double *v, double out[4]) {
   if (!d || !u || !v || !out) return EG_ERR_INVALID;

@@ -316,6 +316,7 @@ void launch_freeze(Ctx &c, const double *u, bool check_admissible) {
   EG_CUDA(cudaMemsetAsync(c.dscal + DS_WAVE, 0, sizeof(double), c.stream));
   const int total = c.nf * c.q;
   const int blocks = (total + 255) / 256;
+  ProfScope ps(c, EG_K_FREEZE, 1);
   EG_DISPATCH_Q(c.q, freeze_kernel<Q><<<blocks, 256, 0, c.stream>>>(
                          c.geo, c.tab, u, c.fa, c.fbb, c.flw, c.frw, c.fpen, c.D, c.derr,
                          reinterpret_cast<unsigned long long *>(c.dscal + DS_WAVE)));
@@ -325,6 +326,7 @@ void launch_freeze(Ctx &c, const double *u, bool check_admissible) {
 void launch_admissible(Ctx &c, const double *u) {
   const int one = 1;
   EG_CUDA(cudaMemcpyAsync(c.derr + 1, &one, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  ProfScope ps(c, EG_K_ADMISSIBLE, 1);
   EG_DISPATCH_Q(c.q, {
     using C = CellCfg<Q>;
     const int blocks = (c.n + C::CPB - 1) / C::CPB;
@@ -334,6 +336,7 @@ void launch_admissible(Ctx &c, const double *u) {
 }
 
 void launch_residual(Ctx &c, const double *u, const double *old, double *r) {
+  ProfScope ps(c, EG_K_RESIDUAL, 1);
   EG_DISPATCH_Q(c.q, {
     using C = CellCfg<Q>;
     const int blocks = (c.n + C::CPB - 1) / C::CPB;
@@ -344,6 +347,7 @@ void launch_residual(Ctx &c, const double *u, const double *old, double *r) {
 }
 
 void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y) {
+  ProfScope ps(c, EG_K_DG_APPLY, 1);
   EG_DISPATCH_Q(c.q, {
     using C = CellCfg<Q>;
     const int blocks = (c.n + C::CPB - 1) / C::CPB;
@@ -366,6 +370,7 @@ static int sm_count() {
 
 void launch_dg_jacobi(Ctx &c, const double *u, bool factor) {
   c.ensure_pc_dg();
+  ProfScope ps(c, EG_K_DG_JACOBI, 1);
   EG_DISPATCH_Q(c.q, {
     constexpr int M = 4 * Q * Q;
     const size_t dyn = dg_block_in_smem<Q>() ? sizeof(double) * M * M : 0;
@@ -383,6 +388,7 @@ void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblock
   const int warps = 8;
   const int grid = (nblocks + warps - 1) / warps;
   const size_t dyn = sizeof(double) * bs * warps;
+  ProfScope ps(c, EG_K_PC_APPLY, 1);
   block_apply_kernel<<<grid, warps * 32, dyn, c.stream>>>(blocks, piv, nblocks, bs, b, x);
   EG_CUDA(cudaGetLastError());
 }

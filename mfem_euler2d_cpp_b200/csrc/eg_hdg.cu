@@ -309,6 +309,7 @@ static int condense_grid(Ctx &c) { return std::min(c.n, sm_count_hdg() * 4); }
 void launch_condense(Ctx &c, const double *u, const double *r) {
   c.ensure_hdg();
   const int grid = condense_grid(c);
+  ProfScope ps(c, EG_K_CONDENSE, 2);
   EG_DISPATCH_Q(c.q, {
     constexpr size_t dyn = condense_dyn_bytes<Q>();
     auto kern = condense_kernel<Q>;
@@ -333,6 +334,7 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
 }
 
 void launch_schur_apply(Ctx &c, const double *v, double *y) {
+  ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
   const int grid = std::min(c.n, sm_count_hdg() * 16);
   EG_DISPATCH_Q(c.q, (cell_gemv_kernel<Q, false><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb,
                                                                             v, c.contrib)));
@@ -344,6 +346,7 @@ void launch_schur_apply(Ctx &c, const double *v, double *y) {
 }
 
 void launch_recover(Ctx &c, const double *lam, double *du) {
+  ProfScope ps(c, EG_K_RECOVER, 1);
   const int grid = std::min(c.n, sm_count_hdg() * 16);
   EG_DISPATCH_Q(c.q, (cell_gemv_kernel<Q, true><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb,
                                                                            lam, du)));
@@ -352,6 +355,7 @@ void launch_recover(Ctx &c, const double *lam, double *du) {
 
 void launch_recovered_residual(Ctx &c, const double *eq, double *er) {
   const int total = c.n * c.p;
+  ProfScope ps(c, EG_K_RECOVERED_RESIDUAL, 1);
   EG_DISPATCH_Q(c.q, (recovered_residual_kernel<Q><<<(total + 255) / 256, 256, 0, c.stream>>>(
                          c.geo, c.tab, c.sf, c.D, eq, er)));
   EG_CUDA(cudaGetLastError());
@@ -359,6 +363,7 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er) {
 
 void launch_schur_jacobi(Ctx &c, bool factor) {
   c.ensure_pc_hdg();
+  ProfScope ps(c, EG_K_SCHUR_JACOBI, 1);
   const int grid = std::min(c.nf, sm_count_hdg() * 32);
   switch (c.t) {
 #define EG_SJ(TT)                                                                                 \

@@ -64,6 +64,29 @@ struct GmresCtl {
 
 struct Ctx;
 
+// Event-timed kernel classes (profiling) and launch counting.
+struct Profiler {
+  bool on = false;
+  struct Rec {
+    int id;
+    long long launches;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> pool;
+  std::vector<Rec> pending;
+  double ms[EG_K_COUNT] = {};
+  long long count[EG_K_COUNT] = {};
+};
+// RAII bracket of the launches of one kernel class on the context stream.
+struct ProfScope {
+  Ctx &c;
+  int id;
+  long long launches;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(Ctx &ctx, int kernel_class, long long nlaunch);
+  ~ProfScope();
+};
+
 // Operators used by the Krylov solver.
 struct LinearOps {
   int N;
@@ -126,6 +149,8 @@ struct Ctx {
 
   bool residual_ready = false;
   bool condensed = false;
+  Profiler prof;
+  long long launches = 0;
 
   void *alloc(size_t bytes);
   template <class T>
@@ -138,6 +163,7 @@ struct Ctx {
   void ensure_pc_hdg();
   void sync();
   void check_device_error();
+  void prof_resolve();
 };
 
 // ---- launchers (eg_cell.cu) ----

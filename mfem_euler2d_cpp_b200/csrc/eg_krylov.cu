@@ -252,6 +252,7 @@ __global__ void fill_kernel(int N, double v, double *__restrict__ out) {
 static int vec_grid(int N) { return std::max(1, std::min((N + 255) / 256, 148 * 16)); }
 
 void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot) {
+  ProfScope ps(c, EG_K_KRYLOV, 1);
   wnorm2_kernel<<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, x, mtab, period, c.partials, c.counter,
                                                           c.dscal + slot);
   EG_CUDA(cudaGetLastError());
@@ -266,6 +267,7 @@ double wnorm(Ctx &c, const double *x, int N, const double *mtab, int period) {
 double cell_norm(Ctx &c, const double *x) { return wnorm(c, x, c.nu, c.mtab_dg, c.m); }
 
 void launch_axpby(Ctx &c, int N, double a, const double *x, double b, const double *y, double *out) {
+  ProfScope ps(c, EG_K_VECTOR, 1);
   axpby_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, a, x, b, y, out);
   EG_CUDA(cudaGetLastError());
 }
@@ -274,6 +276,7 @@ void launch_copy(Ctx &c, int N, const double *x, double *out) {
     EG_CUDA(cudaMemcpyAsync(out, x, sizeof(double) * N, cudaMemcpyDeviceToDevice, c.stream));
 }
 void launch_fill(Ctx &c, int N, double v, double *out) {
+  ProfScope ps(c, EG_K_VECTOR, 1);
   fill_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, v, out);
   EG_CUDA(cudaGetLastError());
 }
@@ -291,6 +294,7 @@ double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, i
     launch_copy(c, N, rhs, res);
   } else {
     ops.apply(c, x, w);
+    ProfScope ps(c, EG_K_VECTOR, 1);
     sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
     EG_CUDA(cudaGetLastError());
   }
@@ -303,14 +307,19 @@ double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, i
   while (iterations < limit) {
     const double beta = residual_norm;
     if (beta <= tol * rhs_norm) break;
-    scale_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, 1 / beta, res, c.V);
-    cycle_init_kernel<<<1, 256, 0, c.stream>>>(c.ctl, R, beta, tol * rhs_norm);
-    EG_CUDA(cudaGetLastError());
+    {
+      ProfScope ps(c, EG_K_KRYLOV, 2);
+      scale_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, 1 / beta, res, c.V);
+      cycle_init_kernel<<<1, 256, 0, c.stream>>>(c.ctl, R, beta, tol * rhs_norm);
+      EG_CUDA(cudaGetLastError());
+    }
     for (int j = 0; j < R && iterations < limit; ++j) {
       const double *vj = c.V + (size_t)j * ldv;
       ops.precondition(c, vj, z);
       ops.apply(c, z, w);
       const int nc = j + 1;
+      {
+      ProfScope ps(c, EG_K_KRYLOV, 5);
       cgs_kernel<0><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
                                                               c.partials, c.counter, c.ctl, R);
       cgs_kernel<1><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
@@ -320,6 +329,7 @@ double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, i
       normalize_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, w, c.V + (size_t)(j + 1) * ldv, c.ctl);
       givens_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
       EG_CUDA(cudaGetLastError());
+      }
       EG_CUDA(cudaMemcpyAsync(&c.hctl->stop, &c.ctl->stop, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                               c.stream));
       c.sync();
@@ -327,14 +337,23 @@ double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, i
       if (c.hctl->err) fail(EG_ERR_GMRES_BREAKDOWN, "GMRES Arnoldi breakdown");
       if (c.hctl->stop) break;
     }
-    backsub_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
-    combine_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.V, ldv, c.ctl, c.kcomb);
-    EG_CUDA(cudaGetLastError());
+    {
+      ProfScope ps(c, EG_K_KRYLOV, 2);
+      backsub_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
+      combine_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.V, ldv, c.ctl, c.kcomb);
+      EG_CUDA(cudaGetLastError());
+    }
     ops.precondition(c, c.kcomb, c.kcorr);
-    add_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.kcorr, x);
+    {
+      ProfScope ps(c, EG_K_VECTOR, 1);
+      add_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.kcorr, x);
+    }
     ops.apply(c, x, w);
-    sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
-    EG_CUDA(cudaGetLastError());
+    {
+      ProfScope ps(c, EG_K_VECTOR, 1);
+      sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
+      EG_CUDA(cudaGetLastError());
+    }
     residual_norm = wnorm(c, res, N, ops.mtab, ops.period);
     if (!std::isfinite(residual_norm)) fail(EG_ERR_GMRES_NONFINITE, "Nonfinite GMRES residual");
   }

@@ -67,6 +67,7 @@ struct Stepper {
   bool keep_stepping() const { return ro.steps > 0 ? step < ro.steps : !final_step; }
 
   void grid_add(double a, const double *x, double *y) {
+    ProfScope ps(c, EG_K_VECTOR, 1);
     add_scaled_kernel<<<std::min((c.nu + 255) / 256, 148 * 16), 256, 0, c.stream>>>(c.nu, a, x, y);
     EG_CUDA(cudaGetLastError());
   }
@@ -137,6 +138,7 @@ struct Stepper {
 
   void end_stage() {
     if (!(converged || ro.newton_steps > 0)) fail(EG_ERR_NEWTON_CONVERGE, "Newton failed to converge");
+    c.launches += 1;
     slope_kernel<<<std::min((c.nu + 255) / 256, 148 * 16), 256, 0, c.stream>>>(c.nu, c.u, stage_base,
                                                                              1. / stage_dt, slope[stage]);
     EG_CUDA(cudaGetLastError());
