@@ -217,8 +217,9 @@ __device__ bool cta_lu_solve(double *A, int lda, double *B, int ldb, int m, int 
         }
       }
       if (lane == 0) {
-        piv[j] = bi;
-        const double pv = A[bi + (size_t)j * lda];
+        // an all-NaN column leaves bi == m: report it as a zero pivot
+        const double pv = bi < m ? A[bi + (size_t)j * lda] : 0.;
+        piv[j] = bi < m ? bi : j;
         bcast[0] = pv;
         inv_piv[j] = 1.0 / pv;
       }

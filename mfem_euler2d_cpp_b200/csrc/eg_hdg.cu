@@ -34,6 +34,137 @@ __host__ __device__ constexpr size_t condense_dyn_bytes() {
 }
 
 // ---------------------------------------------------------- condensation
+// Per-cell staging shared by both condensation kernels.
+template <int Q>
+struct CondenseShared {
+  static constexpr int M = 4 * Q * Q;
+  STab<Q> st;
+  double us[M], UT[16 * Q], FM[4 * Q * 16], SF[4 * Q], CB[4 * Q * 16];
+  int piv_s[M];
+  double inv_piv[M];
+  double bcast[2];
+};
+
+// Assemble the cell system: A (m x m) and [B | r_e] (m x (4t+1)), both
+// column-major with leading dimension m; also store C and the B scalars.
+template <int Q>
+__device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen &fz,
+                               const double *__restrict__ u, const double *__restrict__ r, double *Cb,
+                               double *sf_out, double *A, double *R, int e) {
+  constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
+  const STab<Q> &st = sh.st;
+  for (int i = threadIdx.x; i < M; i += blockDim.x) sh.us[i] = u[(size_t)e * M + i];
+  __syncthreads();
+  for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
+    const int s = task / Q, j = task % Q;
+    double o[4] = {0., 0., 0., 0.};
+    for (int l = 0; l < Q; ++l) {
+      const double f = st.fb(s, j, l);
+      const double *v = sh.us + 4 * line_node<Q>(s, j, l);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) o[c] += f * v[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) sh.UT[task * 4 + c] = o[c];
+  }
+  __syncthreads();
+  // HDG face matrices (src/problem.cpp:661-699): derivative = sign J(U_own)
+  // + stab I with stab = a (own left) or b (own right); C = -ew derivative;
+  // B lift scalar = -dt len/|K| ew (a or b) (problem.cpp:622-630).
+  for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
+    const int s = task / Q, j = task % Q;
+    const bool L = side_is_left(s);
+    const int f = cell_face(e, s, g.nx, g.ny);
+    const int fi = f * Q + j;
+    const double stab = L ? fz.a[fi] : fz.b[fi];
+    double jm[16];
+    jacobian(sh.UT + 4 * task, s < 2 ? 0 : 1, g.gm1, jm);
+    const double nsign = L ? 1. : -1.;
+    const double ewj = st.ew(j);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const double v = nsign * jm[k] + ((k % 5) == 0 ? stab : 0.);
+      sh.FM[task * 16 + k] = v;
+      const double cv = -ewj * v;
+      sh.CB[task * 16 + k] = cv;
+      Cb[((size_t)e * 4 * Q + task) * 16 + k] = cv;
+    }
+    const double len = s < 2 ? g.hy : g.hx;
+    const double scale = g.dt * len / g.area * ewj;
+    const double sv = -scale * stab;
+    sh.SF[task] = sv;
+    sf_out[(size_t)e * 4 * Q + task] = sv;
+  }
+  __syncthreads();
+  build_cell_matrix<Q>(A, M, st, sh.us, sh.FM, g);
+  for (int col = threadIdx.x; col < NR; col += blockDim.x) {
+    double *rc = R + (size_t)col * M;
+    if (col < 4 * T) {
+      for (int i = 0; i < M; ++i) rc[i] = 0.;
+      const int s = col / T, jj = (col % T) >> 2, c = col & 3;
+      const double sv = sh.SF[s * Q + jj];
+      for (int l = 0; l < Q; ++l) {
+        const int i = line_node<Q>(s, jj, l);
+        rc[4 * i + c] = st.fb(s, jj, l) * st.inv_mass(i) * sv;
+      }
+    } else {
+      for (int i = 0; i < M; ++i) rc[i] = r[(size_t)e * M + i];
+    }
+  }
+}
+
+// Outputs of a solved cell: X|y to XY (unless already there), rhs
+// contributions C_e y_e (src/condensation.cpp:141-142) and the Schur Jacobi
+// panels C_s X_s (src/operators.cpp:7-26, 295-301).
+template <int Q>
+__device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, bool copy_out, double *XY,
+                                  double *contrib, double *panels, int e) {
+  constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
+  const STab<Q> &st = sh.st;
+  if (copy_out) {
+    double *dst = XY + (size_t)e * M * NR;
+    for (int i = threadIdx.x; i < M * NR; i += blockDim.x) dst[i] = R[i];
+  }
+  const double *y = R + (size_t)(4 * T) * M;
+  for (int o = threadIdx.x; o < 4 * T; o += blockDim.x) {
+    const int s = o / T, jj = (o % T) >> 2, c = o & 3;
+    double val[4] = {0., 0., 0., 0.};
+    for (int l = 0; l < Q; ++l) {
+      const double f = st.fb(s, jj, l);
+      const double *yv = y + 4 * line_node<Q>(s, jj, l);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) val[d] += f * yv[d];
+    }
+    const double *cb = sh.CB + (s * Q + jj) * 16;
+    double res = 0.;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
+    contrib[(size_t)e * 4 * T + o] = res;
+  }
+  if (panels) {
+    for (int o = threadIdx.x; o < 4 * T * T; o += blockDim.x) {
+      const int s = o / (T * T), rem = o % (T * T);
+      const int row = rem % T, cc = rem / T;
+      const int jj = row >> 2, c = row & 3;
+      const double *xc = R + (size_t)(s * T + cc) * M;
+      double val[4] = {0., 0., 0., 0.};
+      for (int l = 0; l < Q; ++l) {
+        const double f = st.fb(s, jj, l);
+        const double *xv = xc + 4 * line_node<Q>(s, jj, l);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) val[d] += f * xv[d];
+      }
+      const double *cb = sh.CB + (s * Q + jj) * 16;
+      double res = 0.;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
+      panels[(size_t)e * 4 * T * T + o] = res;
+    }
+  }
+}
+
+// Generic condensation (any degree): CTA-cooperative LU on shared or global
+// memory (StreamCondense, src/condensation.cpp:131-148).
 template <int Q>
 __global__ void __launch_bounds__(256)
     condense_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
@@ -41,123 +172,222 @@ __global__ void __launch_bounds__(256)
                     double *contrib, double *panels, double *work, int *err) {
   constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
   constexpr int MODE = condense_mode<Q>();
-  __shared__ STab<Q> st;
-  __shared__ double us[M], UT[16 * Q], FM[4 * Q * 16], SF[4 * Q], CB[4 * Q * 16];
-  __shared__ int piv_s[M];
-  __shared__ double inv_piv[M];
-  __shared__ double bcast[2];
+  __shared__ CondenseShared<Q> sh;
   extern __shared__ double dyn[];
-  load_tables<Q>(st, tab);
+  load_tables<Q>(sh.st, tab);
   for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < M; i += blockDim.x) us[i] = u[(size_t)e * M + i];
-    __syncthreads();
-    for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
-      const int s = task / Q, j = task % Q;
-      double o[4] = {0., 0., 0., 0.};
-      for (int l = 0; l < Q; ++l) {
-        const double f = st.fb(s, j, l);
-        const double *v = us + 4 * line_node<Q>(s, j, l);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) o[c] += f * v[c];
-      }
-#pragma unroll
-      for (int c = 0; c < 4; ++c) UT[task * 4 + c] = o[c];
-    }
-    __syncthreads();
-    // HDG face matrices (src/problem.cpp:661-699): derivative = sign J(U_own)
-    // + stab I with stab = a (own left) or b (own right); C = -ew derivative;
-    // B lift scalar = -dt len/|K| ew (a or b) (problem.cpp:622-630).
-    for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
-      const int s = task / Q, j = task % Q;
-      const bool L = side_is_left(s);
-      const int f = cell_face(e, s, g.nx, g.ny);
-      const int fi = f * Q + j;
-      const double stab = L ? fz.a[fi] : fz.b[fi];
-      double jm[16];
-      jacobian(UT + 4 * task, s < 2 ? 0 : 1, g.gm1, jm);
-      const double nsign = L ? 1. : -1.;
-      const double ewj = st.ew(j);
-#pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const double v = nsign * jm[k] + ((k % 5) == 0 ? stab : 0.);
-        FM[task * 16 + k] = v;
-        const double cv = -ewj * v;
-        CB[task * 16 + k] = cv;
-        Cb[((size_t)e * 4 * Q + task) * 16 + k] = cv;
-      }
-      const double len = s < 2 ? g.hy : g.hx;
-      const double scale = g.dt * len / g.area * ewj;
-      const double sv = -scale * stab;
-      SF[task] = sv;
-      sf_out[(size_t)e * 4 * Q + task] = sv;
-    }
     __syncthreads();
     double *A = MODE < 2 ? dyn : work + (size_t)blockIdx.x * M * M;
     double *R = MODE == 0 ? dyn + (size_t)M * M : XY + (size_t)e * M * NR;
-    build_cell_matrix<Q>(A, M, st, us, FM, g);
-    for (int col = threadIdx.x; col < NR; col += blockDim.x) {
-      double *rc = R + (size_t)col * M;
-      if (col < 4 * T) {
-        for (int i = 0; i < M; ++i) rc[i] = 0.;
-        const int s = col / T, jj = (col % T) >> 2, c = col & 3;
-        const double sv = SF[s * Q + jj];
-        for (int l = 0; l < Q; ++l) {
-          const int i = line_node<Q>(s, jj, l);
-          rc[4 * i + c] = st.fb(s, jj, l) * st.inv_mass(i) * sv;
-        }
-      } else {
-        for (int i = 0; i < M; ++i) rc[i] = r[(size_t)e * M + i];
-      }
-    }
+    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, A, R, e);
     __syncthreads();
-    const bool ok = cta_lu_solve<(M + 31) / 32>(A, M, R, M, M, NR, piv_s, inv_piv, bcast);
+    const bool ok = cta_lu_solve<(M + 31) / 32>(A, M, R, M, M, NR, sh.piv_s, sh.inv_piv, sh.bcast);
     if (!ok) {
       if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
       continue;
     }
-    if (MODE == 0) {
-      double *dst = XY + (size_t)e * M * NR;
-      for (int i = threadIdx.x; i < M * NR; i += blockDim.x) dst[i] = R[i];
-    }
-    // rhs contributions C_e y_e (src/condensation.cpp:141-142)
-    const double *y = R + (size_t)(4 * T) * M;
-    for (int o = threadIdx.x; o < 4 * T; o += blockDim.x) {
-      const int s = o / T, jj = (o % T) >> 2, c = o & 3;
-      double val[4] = {0., 0., 0., 0.};
-      for (int l = 0; l < Q; ++l) {
-        const double f = st.fb(s, jj, l);
-        const double *yv = y + 4 * line_node<Q>(s, jj, l);
+    condense_epilogue<Q>(sh, R, MODE == 0, XY, contrib, panels, e);
+  }
+}
+
+// Register-resident condensation for cells whose augmented system
+// [A | B | r] (m x (m + 4t + 1)) fits the register file of one CTA.
+// The system is staged in shared memory, then held in registers in a 2-D
+// block-cyclic layout over a TR x TC thread grid: thread (tr, tc) owns rows
+// tr + i*TR and columns tc + k*TC. Each elimination step broadcasts the
+// pivot column and the new pivot row through double-buffered shared
+// memory (two barriers per step; every warp finds the pivot itself), then
+// every thread updates its block of the trailing matrix with FMAs on
+// registers. Pivoting is partial by rows with the first maximum winning,
+// multipliers are a_ij * (1/pivot), and the upper solve divides by the
+// pivot, as in MFEM LUFactors::Factor/Solve. Back substitution runs on the
+// right-hand-side columns in registers (one barrier per step).
+template <int Q, int TR, int TC>
+struct RegCfg {
+  static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, NC = M + NR;
+  static constexpr int RP = (M + TR - 1) / TR, CP = (NC + TC - 1) / TC;
+  static constexpr int THREADS = TR * TC;
+};
+
+template <int Q, int TR, int TC, int MINB>
+__global__ void __launch_bounds__(TR *TC, MINB)
+    condense_reg_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                        const double *__restrict__ r, double *XY, double *Cb, double *sf_out,
+                        double *contrib, double *panels, int *err) {
+  using C = RegCfg<Q, TR, TC>;
+  constexpr int M = C::M, NC = C::NC, RP = C::RP, CP = C::CP;
+  __shared__ CondenseShared<Q> sh;
+  __shared__ double colbuf[2][M], rowbuf[2][NC], rowold[2][NC];
+  extern __shared__ double dyn[];  // augmented system, column-major M x NC
+  const int tr = threadIdx.x % TR, tc = threadIdx.x / TR;
+  const int lane = threadIdx.x & 31;
+  load_tables<Q>(sh.st, tab);
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, dyn, dyn + (size_t)M * M, e);
+    __syncthreads();
+    double a[RP][CP];
 #pragma unroll
-        for (int d = 0; d < 4; ++d) val[d] += f * yv[d];
+    for (int i = 0; i < RP; ++i) {
+      const int row = tr + i * TR;
+#pragma unroll
+      for (int k = 0; k < CP; ++k) {
+        const int col = tc + k * TC;
+        a[i][k] = (row < M && col < NC) ? dyn[row + (size_t)col * M] : 0.;
       }
-      const double *cb = CB + (s * Q + jj) * 16;
-      double res = 0.;
-#pragma unroll
-      for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
-      contrib[(size_t)e * 4 * T + o] = res;
     }
-    // Schur Jacobi panels C_s X_s (src/operators.cpp:7-26, 295-301)
-    if (panels) {
-      for (int o = threadIdx.x; o < 4 * T * T; o += blockDim.x) {
-        const int s = o / (T * T), rem = o % (T * T);
-        const int row = rem % T, cc = rem / T;
-        const int jj = row >> 2, c = row & 3;
-        const double *xc = R + (size_t)(s * T + cc) * M;
-        double val[4] = {0., 0., 0., 0.};
-        for (int l = 0; l < Q; ++l) {
-          const double f = st.fb(s, jj, l);
-          const double *xv = xc + 4 * line_node<Q>(s, jj, l);
+    bool singular = false;
+    for (int j = 0; j < M; ++j) {
+      const int buf = j & 1;
+      const int jk = j / TC, ji = j / TR;
+      if (tc == j % TC) {
 #pragma unroll
-          for (int d = 0; d < 4; ++d) val[d] += f * xv[d];
+        for (int i = 0; i < RP; ++i) {
+          const int row = tr + i * TR;
+          if (row >= j && row < M) {
+            double v = 0.;
+#pragma unroll
+            for (int k = 0; k < CP; ++k)
+              if (k == jk) v = a[i][k];
+            colbuf[buf][row] = v;
+          }
         }
-        const double *cb = CB + (s * Q + jj) * 16;
-        double res = 0.;
+      }
+      __syncthreads();
+      double best = -1.;
+      int bi = M;
+      for (int i = j + lane; i < M; i += 32) {
+        const double v = fabs(colbuf[buf][i]);
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
 #pragma unroll
-        for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
-        panels[(size_t)e * 4 * T * T + o] = res;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      const int p = bi < M ? bi : j;  // an all-NaN column leaves bi == M
+      const double pv = bi < M ? colbuf[buf][p] : 0.;
+      if (!(fabs(pv) > 0.)) {
+        singular = true;
+        break;
+      }
+      const double inv = 1.0 / pv;
+      const int pi = p / TR;
+      if (tr == j % TR || tr == p % TR) {
+#pragma unroll
+        for (int k = 0; k < CP; ++k) {
+          const int col = tc + k * TC;
+          if (col < NC) {
+            double vj = 0., vp = 0.;
+#pragma unroll
+            for (int i = 0; i < RP; ++i) {
+              if (i == ji) vj = a[i][k];
+              if (i == pi) vp = a[i][k];
+            }
+            if (tr == j % TR) rowold[buf][col] = vj;
+            if (tr == p % TR) rowbuf[buf][col] = vp;
+          }
+        }
+      }
+      __syncthreads();
+      if (p != j && (tr == j % TR || tr == p % TR)) {
+#pragma unroll
+        for (int k = 0; k < CP; ++k) {
+          const int col = tc + k * TC;
+          if (col < NC) {
+#pragma unroll
+            for (int i = 0; i < RP; ++i) {
+              if (tr == j % TR && i == ji) a[i][k] = rowbuf[buf][col];
+              if (tr == p % TR && i == pi) a[i][k] = rowold[buf][col];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < RP; ++i) {
+        const int row = tr + i * TR;
+        if (row > j && row < M) {
+          const double l = (row == p ? colbuf[buf][j] : colbuf[buf][row]) * inv;
+#pragma unroll
+          for (int k = 0; k < CP; ++k) {
+            const int col = tc + k * TC;
+            if (col > j && col < NC) {
+              a[i][k] -= l * rowbuf[buf][col];
+            } else if (col == j) {
+              a[i][k] = l;
+            }
+          }
+        }
       }
     }
+    if (singular) {
+      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
+      continue;
+    }
+    // U to shared memory for the back substitution
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int row = tr + i * TR;
+#pragma unroll
+      for (int k = 0; k < CP; ++k) {
+        const int col = tc + k * TC;
+        if (row < M && col < M) dyn[row + (size_t)col * M] = a[i][k];
+      }
+    }
+    __syncthreads();
+    for (int j = M - 1; j >= 0; --j) {
+      const int buf = j & 1;
+      const double ujj = dyn[j + (size_t)j * M];
+      if (tr == j % TR) {
+        const int ji = j / TR;
+#pragma unroll
+        for (int i = 0; i < RP; ++i) {
+          if (i == ji) {
+#pragma unroll
+            for (int k = 0; k < CP; ++k) {
+              const int col = tc + k * TC;
+              if (col >= M && col < NC) {
+                const double x = a[i][k] / ujj;
+                a[i][k] = x;
+                rowbuf[buf][col] = x;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < RP; ++i) {
+        const int row = tr + i * TR;
+        if (row < j) {
+          const double uij = dyn[row + (size_t)j * M];
+#pragma unroll
+          for (int k = 0; k < CP; ++k) {
+            const int col = tc + k * TC;
+            if (col >= M && col < NC) a[i][k] -= uij * rowbuf[buf][col];
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int row = tr + i * TR;
+#pragma unroll
+      for (int k = 0; k < CP; ++k) {
+        const int col = tc + k * TC;
+        if (row < M && col >= M && col < NC) dyn[row + (size_t)col * M] = a[i][k];
+      }
+    }
+    __syncthreads();
+    condense_epilogue<Q>(sh, dyn + (size_t)M * M, true, XY, contrib, panels, e);
   }
 }
 
@@ -306,24 +536,44 @@ static int sm_count_hdg() {
 
 static int condense_grid(Ctx &c) { return std::min(c.n, sm_count_hdg() * 4); }
 
+template <int Q, int TR, int TC, int MINB>
+static void launch_condense_reg(Ctx &c, const double *u, const double *r) {
+  using C = RegCfg<Q, TR, TC>;
+  constexpr size_t dyn = sizeof(double) * (size_t)C::M * C::NC;
+  auto kern = condense_reg_kernel<Q, TR, TC, MINB>;
+  if (dyn > 48 * 1024)
+    EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  const int grid = std::min(c.n, sm_count_hdg() * MINB);
+  kern<<<grid, C::THREADS, dyn, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, r,
+                                            c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
+}
+
 void launch_condense(Ctx &c, const double *u, const double *r) {
   c.ensure_hdg();
   const int grid = condense_grid(c);
   ProfScope ps(c, EG_K_CONDENSE, 2);
-  EG_DISPATCH_Q(c.q, {
-    constexpr size_t dyn = condense_dyn_bytes<Q>();
-    auto kern = condense_kernel<Q>;
-    if (dyn > 48 * 1024)
-      EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    if (condense_mode<Q>() == 2 && (c.work_cell == nullptr || c.work_slots < grid)) {
-      constexpr int M = 4 * Q * Q;
-      c.work_cell = c.alloc_n<double>((size_t)grid * M * M);
-      c.work_slots = grid;
-    }
-    kern<<<grid, 256, dyn, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u,
-                                       r, c.XY, c.Cb, c.sf, c.contrib, c.panels, c.work_cell,
-                                       c.derr);
-  });
+  switch (c.q) {
+    case 1: launch_condense_reg<1, 4, 8, 4>(c, u, r); break;
+    case 2: launch_condense_reg<2, 8, 8, 4>(c, u, r); break;
+    case 3: launch_condense_reg<3, 8, 16, 3>(c, u, r); break;
+    case 4: launch_condense_reg<4, 16, 16, 2>(c, u, r); break;
+    case 5: launch_condense_reg<5, 16, 24, 1>(c, u, r); break;
+    default:
+      EG_DISPATCH_Q(c.q, {
+        constexpr size_t dyn = condense_dyn_bytes<Q>();
+        auto kern = condense_kernel<Q>;
+        if (dyn > 48 * 1024)
+          EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        if (condense_mode<Q>() == 2 && (c.work_cell == nullptr || c.work_slots < grid)) {
+          constexpr int M = 4 * Q * Q;
+          c.work_cell = c.alloc_n<double>((size_t)grid * M * M);
+          c.work_slots = grid;
+        }
+        kern<<<grid, 256, dyn, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u,
+                                           r, c.XY, c.Cb, c.sf, c.contrib, c.panels, c.work_cell,
+                                           c.derr);
+      });
+  }
   EG_CUDA(cudaGetLastError());
   // rhs_f = contrib_L + contrib_R (s.rhs = 0; rhs[ids] += C y)
   const int blocks = (c.nl + 255) / 256;
