@@ -80,7 +80,8 @@ enum eg_slot {
   EG_SLOT_D = 6,       /* HDG trace diagonal D (nl) */
   EG_SLOT_X = 7,       /* HDG responses X, n blocks of m x 4t column-major */
   EG_SLOT_Y = 8,       /* HDG particular responses y (nu) */
-  EG_SLOT_PC_BLOCKS = 9, /* preconditioner blocks (DG: n*m*m, HDG: nf*t*t), column-major */
+  EG_SLOT_PC_BLOCKS = 9, /* preconditioner blocks (DG: n*m*m, HDG: nf*t*t), column-major;
+                          after eg_pc_factor(ctx, 1): DG packed pivoted LU, HDG explicit inverse */
   EG_SLOT_HLL_A = 10,  /* frozen left HLL bound per face point (nf*q) */
   EG_SLOT_HLL_B = 11,  /* frozen right HLL bound per face point (nf*q) */
   EG_SLOT_COUNT = 12

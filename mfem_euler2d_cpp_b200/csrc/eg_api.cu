@@ -180,7 +180,7 @@ struct HdgOps : LinearOps {
   }
   void apply(Ctx &c, const double *x, double *y) override { launch_schur_apply(c, x, y); }
   void precondition(Ctx &c, const double *b, double *x) override {
-    launch_block_apply(c, c.pc_hdg, c.piv_hdg, c.nf, c.t, b, x);
+    launch_block_inverse_apply(c, c.pc_hdg, c.nf, c.t, b, x);
   }
 };
 
@@ -748,7 +748,7 @@ int eg_pc_apply(eg_ctx *ctx, const double *b, double *x) {
     } else {
       if (!c.pc_hdg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
       eg::upload_vec(c, c.tmp_trace, b, c.nl);
-      eg::launch_block_apply(c, c.pc_hdg, c.piv_hdg, c.nf, c.t, c.tmp_trace, c.lam);
+      eg::launch_block_inverse_apply(c, c.pc_hdg, c.nf, c.t, c.tmp_trace, c.lam);
       eg::download_vec(c, x, c.lam, c.nl);
     }
   });

@@ -50,7 +50,7 @@ struct CondenseShared {
 template <int Q>
 __device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen &fz,
                                const double *__restrict__ u, const double *__restrict__ r, double *Cb,
-                               double *sf_out, double *A, double *R, int e) {
+                               double *sf_out, double *A, double *R, int e, int ld = 4 * Q * Q) {
   constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
   const STab<Q> &st = sh.st;
   for (int i = threadIdx.x; i < M; i += blockDim.x) sh.us[i] = u[(size_t)e * M + i];
@@ -96,9 +96,9 @@ __device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen
     sf_out[(size_t)e * 4 * Q + task] = sv;
   }
   __syncthreads();
-  build_cell_matrix<Q>(A, M, st, sh.us, sh.FM, g);
+  build_cell_matrix<Q>(A, ld, st, sh.us, sh.FM, g);
   for (int col = threadIdx.x; col < NR; col += blockDim.x) {
-    double *rc = R + (size_t)col * M;
+    double *rc = R + (size_t)col * ld;
     if (col < 4 * T) {
       for (int i = 0; i < M; ++i) rc[i] = 0.;
       const int s = col / T, jj = (col % T) >> 2, c = col & 3;
@@ -391,6 +391,283 @@ __global__ void __launch_bounds__(TR *TC, MINB)
   }
 }
 
+// ------------------------------------------- tensor-core Gauss-Jordan
+// D = C + A B on the FP64 tensor pipe: m8n8k4, A row-major 8x4 (one element
+// per lane: row lane/4, column lane%4), B column-major 4x8 (row lane%4,
+// column lane/4), C/D 8x8 (two elements per lane: row lane/4, columns
+// 2*(lane%4) and 2*(lane%4)+1).
+__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int Q, int WR, int WC>
+struct GjCfg {
+  static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, NC = M + NR;
+  static constexpr int MT = (M + 7) / 8, NT = (NC + 7) / 8;
+  static constexpr int TRW = (MT + WR - 1) / WR, TCW = (NT + WC - 1) / WC;
+  static constexpr int MP = 8 * TRW * WR, NP = 8 * TCW * WC;  // padded to whole warp tile grids
+  static constexpr int THREADS = 32 * WR * WC;
+  static constexpr int LD = M + 1;           // odd staging stride: conflict-free columns
+  static constexpr int KR = (M + 31) / 32;   // rows per lane in the pivot search
+};
+
+// Blocked Gauss-Jordan condensation on the tensor cores. The augmented cell
+// system W = [A | B | r_e] lives in registers as 8x8 accumulator tiles; warp
+// (wr, wc) owns tiles (wr + a*WR, wc + b*WC) of a tile grid padded with zero
+// rows and columns to whole warp grids. Panels are 4 columns wide:
+//  * the 4 pivot rows of panel p publish their trailing columns W_top;
+//  * one m8n8k4 MMA per trailing tile applies W_i -= A_i T^{-1} W_top with
+//    the A operand A_i = W_i[panel] for ordinary rows and A_i = T_r - e_r for
+//    pivot row r, which turns the same MMA into the row normalisation
+//    W_r -> (T^{-1} W_top)_r; B fragments T^{-1} W_top are formed per lane;
+//  * the tile column holding panel p+1 (always the first trailing one) is
+//    staged right after its MMAs, and warp 0 selects the pivots of panel
+//    p+1 while the tensor pipe drains the rest of panel p.
+// Pivot selection is partial pivoting over the rows not yet used: largest
+// magnitude after eliminating the panel's earlier pivots with multipliers
+// a_ij * (1/pivot), first row on ties (MFEM LUFactors::Factor), found with
+// warp max/min reductions on the IEEE bit pattern. Pivoting is virtual (rows
+// never move): after the last panel, row pivrow[j] holds unknown j, so the
+// right-hand-side columns hold X_e = A_e^{-1} B_e and y_e = A_e^{-1} r_e,
+// permuted back on the way out (StreamCondense, src/condensation.cpp:136-140,
+// carried to reduced row echelon form: no triangular solve follows).
+template <int Q, int WR, int WC, int MINB>
+__global__ void __launch_bounds__(32 * WR *WC, MINB)
+    condense_gj_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                       const double *__restrict__ r, double *XY, double *Cb, double *sf_out,
+                       double *contrib, double *panels, int *err) {
+  using C = GjCfg<Q, WR, WC>;
+  constexpr int M = C::M, NC = C::NC, MP = C::MP, NP = C::NP;
+  constexpr int TRW = C::TRW, TCW = C::TCW, LD = C::LD, KR = C::KR, NPAN = M / 4;
+  __shared__ CondenseShared<Q> sh;
+  __shared__ double pan[2][MP][4], top[2][4][NP];
+  __shared__ double fac[2][16];   // T^{-1} of the panel's pivot block, row-major 4x4
+  __shared__ double lmul[MP][3];  // multipliers of every row during pivot selection
+  __shared__ int pivs[2][4];
+  __shared__ int invp[MP];
+  __shared__ unsigned char used[MP];
+  __shared__ int sing;
+  extern __shared__ double dyn[];  // staged system, column-major M x NC, stride LD
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = warp % WR, wc = warp / WR;
+  const int gq = lane >> 2, tq = lane & 3;
+  load_tables<Q>(sh.st, tab);
+
+  // Warp 0: choose the 4 pivots of the panel staged in pan[buf]; publish
+  // T^{-1} and turn the pivot rows of the A operand into T_r - e_r.
+  auto select = [&](int jbase, int buf) {
+    double w[KR][4];
+    bool un[KR];
+#pragma unroll
+    for (int k = 0; k < KR; ++k) {
+      const int i = lane + 32 * k;
+      un[k] = i < M && !used[i];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) w[k][c] = un[k] ? pan[buf][i][c] : 0.;
+    }
+    int prow[4];
+    double U[4][4], dinv[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      unsigned hi = 0u, lo = 0u;
+      int idx = 0x7fffffff;
+      double best = -1.;
+#pragma unroll
+      for (int k = 0; k < KR; ++k) {
+        const double v = fabs(w[k][jj]);
+        if (un[k] && v > best) {  // NaN never wins, as in the reference's comparison
+          best = v;
+          idx = lane + 32 * k;
+        }
+      }
+      if (best >= 0.) {
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(best);
+        hi = (unsigned)(bits >> 32);
+        lo = (unsigned)bits;
+      }
+      const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+      const bool c1 = hi == mhi && idx != 0x7fffffff;
+      const unsigned mlo = __reduce_max_sync(0xffffffffu, c1 ? lo : 0u);
+      const bool c2 = c1 && lo == mlo;
+      const int bi = (int)__reduce_min_sync(0xffffffffu, c2 ? (unsigned)idx : 0x7fffffffu);
+      if ((mhi == 0u && mlo == 0u) || bi >= M) return false;
+      prow[jj] = bi;
+      const int owner = bi & 31, kk = bi >> 5;
+      double pw[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        double v = 0.;
+#pragma unroll
+        for (int k = 0; k < KR; ++k)
+          if (k == kk) v = w[k][c];
+        pw[c] = __shfl_sync(0xffffffffu, v, owner);
+      }
+#pragma unroll
+      for (int k = 0; k < KR; ++k)
+        if (k == kk && lane == owner) un[k] = false;
+      const double inv = __drcp_rn(pw[jj]);
+      dinv[jj] = inv;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) U[jj][c] = pw[c];
+      if (jj < 3) {
+#pragma unroll
+        for (int k = 0; k < KR; ++k) {
+          if (un[k]) {
+            const double l = w[k][jj] * inv;
+            lmul[lane + 32 * k][jj] = l;
+#pragma unroll
+            for (int c = jj + 1; c < 4; ++c) w[k][c] -= l * pw[c];
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // T^{-1}: lane c < 4 solves T x = e_c with the factors (L from lmul, U, 1/pivots)
+    if (lane < 4) {
+      double y[4];
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr) {
+        double v = rr == lane ? 1. : 0.;
+#pragma unroll
+        for (int cc = 0; cc < rr; ++cc) v -= lmul[prow[rr]][cc] * y[cc];
+        y[rr] = v;
+      }
+#pragma unroll
+      for (int rr = 3; rr >= 0; --rr) {
+        double v = y[rr];
+#pragma unroll
+        for (int cc = rr + 1; cc < 4; ++cc) v -= U[rr][cc] * y[cc];
+        y[rr] = v * dinv[rr];
+      }
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr) fac[buf][rr * 4 + lane] = y[rr];
+    }
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) {
+      if (lane == rr) {
+        pivs[buf][rr] = prow[rr];
+        used[prow[rr]] = 1;
+        invp[prow[rr]] = jbase + rr;
+        pan[buf][prow[rr]][rr] -= 1.;  // A operand T_r - e_r
+      }
+    }
+    return true;
+  };
+
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, dyn, dyn + (size_t)LD * M, e, LD);
+    for (int i = threadIdx.x; i < MP; i += C::THREADS) {
+      used[i] = i >= M ? 1 : 0;
+      invp[i] = 0;
+    }
+    if (threadIdx.x == 0) sing = 0;
+    __syncthreads();
+    double acc[TRW][TCW][2];
+#pragma unroll
+    for (int a = 0; a < TRW; ++a) {
+      const int row = (wr + a * WR) * 8 + gq;
+#pragma unroll
+      for (int b = 0; b < TCW; ++b) {
+        const int col = (wc + b * WC) * 8 + 2 * tq;
+        acc[a][b][0] = (row < M && col < NC) ? dyn[row + (size_t)col * LD] : 0.;
+        acc[a][b][1] = (row < M && col + 1 < NC) ? dyn[row + (size_t)(col + 1) * LD] : 0.;
+      }
+    }
+    // stage panel 0 (tile column 0, left half)
+    if (wc == 0 && tq < 2) {
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int row = (wr + a * WR) * 8 + gq;
+        pan[0][row][2 * tq] = acc[a][0][0];
+        pan[0][row][2 * tq + 1] = acc[a][0][1];
+      }
+    }
+    __syncthreads();
+    if (warp == 0 && !select(0, 0) && lane == 0) sing = 1;
+    __syncthreads();
+#pragma unroll 1
+    for (int p = 0; p < NPAN && !sing; ++p) {
+      const int j = 4 * p, pb = p & 1;
+      const int pr0 = pivs[pb][0], pr1 = pivs[pb][1], pr2 = pivs[pb][2], pr3 = pivs[pb][3];
+      const int tstart = (j + 4) >> 3;  // first tile column holding columns >= j+4 (= panel p+1's)
+      // publish the trailing columns of the pivot rows (zero left of j+4)
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int row = (wr + a * WR) * 8 + gq;
+        const int rr = row == pr0 ? 0 : row == pr1 ? 1 : row == pr2 ? 2 : row == pr3 ? 3 : -1;
+        if (rr >= 0) {
+#pragma unroll
+          for (int b = 0; b < TCW; ++b) {
+            const int tj = wc + b * WC;
+            if (tj >= tstart) {
+              const int col = tj * 8 + 2 * tq;
+              top[pb][rr][col] = col >= j + 4 ? acc[a][b][0] : 0.;
+              top[pb][rr][col + 1] = col + 1 >= j + 4 ? acc[a][b][1] : 0.;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      // A operands (row gq, column tq of each tile row) and B operands
+      // (row tq, column gq of each tile column) = T^{-1} top
+      double af[TRW];
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) af[a] = -pan[pb][(wr + a * WR) * 8 + gq][tq];
+      const double *F = fac[pb];
+      const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
+      const bool more = p + 1 < NPAN;
+      const int jn = j + 4, half = (jn >> 2) & 1, nb = pb ^ 1;
+      const bool stager = more && wc == tstart % WC && (tq >> 1) == half;
+#pragma unroll
+      for (int b = 0; b < TCW; ++b) {
+        const int tj = wc + b * WC;
+        if (tj >= tstart) {
+          const int col = tj * 8 + gq;
+          const double bf = f0 * top[pb][0][col] + f1 * top[pb][1][col] + f2 * top[pb][2][col] +
+                            f3 * top[pb][3][col];
+#pragma unroll
+          for (int a = 0; a < TRW; ++a) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf);
+          if (tj == tstart && stager) {
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) {
+              const int row = (wr + a * WR) * 8 + gq;
+              pan[nb][row][2 * (tq & 1)] = acc[a][b][0];
+              pan[nb][row][2 * (tq & 1) + 1] = acc[a][b][1];
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (more && warp == 0 && !select(jn, nb) && lane == 0) sing = 1;
+      __syncthreads();
+    }
+    if (sing) {
+      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
+      continue;
+    }
+    // right-hand sides back to unknown order: R(invp[w], col) = W(w, M + col)
+    double *R = dyn;  // compact M x NR, stride M (the staged system is no longer needed)
+#pragma unroll
+    for (int a = 0; a < TRW; ++a) {
+      const int row = (wr + a * WR) * 8 + gq;
+      if (row < M) {
+        const int jrow = invp[row];
+#pragma unroll
+        for (int b = 0; b < TCW; ++b) {
+          const int col = (wc + b * WC) * 8 + 2 * tq;
+          if (col >= M && col < NC) R[(size_t)(col - M) * M + jrow] = acc[a][b][0];
+          if (col + 1 >= M && col + 1 < NC) R[(size_t)(col + 1 - M) * M + jrow] = acc[a][b][1];
+        }
+      }
+    }
+    __syncthreads();
+    condense_epilogue<Q>(sh, R, true, XY, contrib, panels, e);
+  }
+}
+
 // -------------------------------------------------- Schur action / recovery
 // Per cell: gather the 4t trace values, mid = X_e v_e (GEMV streaming X once),
 // then either restrict with C (Schur action, src/operators.cpp:166-178) or
@@ -487,14 +764,17 @@ __global__ void __launch_bounds__(256)
   for (int c = 0; c < 4; ++c) er[(size_t)e * M + 4 * node + c] = -acc[c];
 }
 
-// Schur block-Jacobi: S_ff = D_f - P_L - P_R, then pivoted LU in place
-// (ElementOperator::DiagonalBlocks src/operators.cpp:275-303 + linear.cpp:198-202).
+// Schur block-Jacobi: S_ff = D_f - P_L - P_R (ElementOperator::DiagonalBlocks
+// src/operators.cpp:275-303). With factor set, the block is inverted through
+// its pivoted LU (LUFactors, src/linear.cpp:198-202) applied to the identity,
+// and the explicit inverse is stored so the preconditioner apply is a
+// coalesced batched GEMV instead of two dependent triangular sweeps.
 template <int T>
 __global__ void __launch_bounds__(64)
     schur_jacobi_kernel(int nx, int ny, int nf, const double *__restrict__ D,
                         const double *__restrict__ panels, double *blocks, int *pivots, bool factor,
                         int *err) {
-  __shared__ double S[T * T];
+  __shared__ double S[T * T], Inv[T * T];
   __shared__ int piv_s[T];
   __shared__ double inv_piv[T];
   __shared__ double bcast[2];
@@ -508,18 +788,32 @@ __global__ void __launch_bounds__(64)
       const int row = o % T, col = o / T;
       const double d = row == col ? D[(size_t)f * T + row] : 0.;
       S[o] = (d - pl[o]) - pr[o];
+      Inv[o] = row == col ? 1. : 0.;
     }
     __syncthreads();
+    const double *out = S;
     if (factor) {
-      const bool ok = cta_lu_solve<(T + 31) / 32>(S, T, nullptr, 1, T, 0, piv_s, inv_piv, bcast);
+      const bool ok = cta_lu_solve<(T + 31) / 32>(S, T, Inv, T, T, T, piv_s, inv_piv, bcast);
       if (!ok && threadIdx.x == 0) raise_err(err, DERR_SINGULAR_JACOBI);
-    } else {
-      for (int i = threadIdx.x; i < T; i += blockDim.x) piv_s[i] = i;
+      out = Inv;
     }
-    __syncthreads();
-    for (int o = threadIdx.x; o < T * T; o += blockDim.x) blocks[(size_t)f * T * T + o] = S[o];
-    for (int i = threadIdx.x; i < T; i += blockDim.x) pivots[(size_t)f * T + i] = piv_s[i];
+    for (int i = threadIdx.x; i < T; i += blockDim.x) pivots[(size_t)f * T + i] = factor ? piv_s[i] : i;
+    for (int o = threadIdx.x; o < T * T; o += blockDim.x) blocks[(size_t)f * T * T + o] = out[o];
   }
+}
+
+// x_b = Inv_b b_b for column-major bs x bs inverses; one thread per output row.
+__global__ void __launch_bounds__(256) block_gemv_kernel(const double *__restrict__ inv, int nblocks, int bs,
+                                                         const double *__restrict__ b,
+                                                         double *__restrict__ x) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (long long)nblocks * bs) return;
+  const int blk = (int)(id / bs), row = (int)(id % bs);
+  const double *ib = inv + (size_t)blk * bs * bs + row;
+  const double *bb = b + (size_t)blk * bs;
+  double acc = 0.;
+  for (int c = 0; c < bs; ++c) acc += ib[(size_t)c * bs] * bb[c];
+  x[id] = acc;
 }
 
 // ================================================================ launchers
@@ -548,16 +842,28 @@ static void launch_condense_reg(Ctx &c, const double *u, const double *r) {
                                             c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
 }
 
+template <int Q, int WR, int WC, int MINB>
+static void launch_condense_gj(Ctx &c, const double *u, const double *r) {
+  using C = GjCfg<Q, WR, WC>;
+  constexpr size_t dyn = sizeof(double) * (size_t)C::LD * C::NC;
+  auto kern = condense_gj_kernel<Q, WR, WC, MINB>;
+  if (dyn > 48 * 1024)
+    EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  const int grid = std::min(c.n, sm_count_hdg() * MINB);
+  kern<<<grid, C::THREADS, dyn, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, r,
+                                            c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
+}
+
 void launch_condense(Ctx &c, const double *u, const double *r) {
   c.ensure_hdg();
   const int grid = condense_grid(c);
   ProfScope ps(c, EG_K_CONDENSE, 2);
   switch (c.q) {
-    case 1: launch_condense_reg<1, 4, 8, 4>(c, u, r); break;
-    case 2: launch_condense_reg<2, 8, 8, 4>(c, u, r); break;
-    case 3: launch_condense_reg<3, 8, 16, 3>(c, u, r); break;
-    case 4: launch_condense_reg<4, 16, 16, 2>(c, u, r); break;
-    case 5: launch_condense_reg<5, 16, 24, 1>(c, u, r); break;
+    case 1: launch_condense_gj<1, 1, 1, 8>(c, u, r); break;
+    case 2: launch_condense_gj<2, 1, 2, 6>(c, u, r); break;
+    case 3: launch_condense_gj<3, 2, 2, 4>(c, u, r); break;
+    case 4: launch_condense_gj<4, 2, 4, 2>(c, u, r); break;
+    case 5: launch_condense_gj<5, 2, 4, 1>(c, u, r); break;
     default:
       EG_DISPATCH_Q(c.q, {
         constexpr size_t dyn = condense_dyn_bytes<Q>();
@@ -608,6 +914,13 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er) {
   ProfScope ps(c, EG_K_RECOVERED_RESIDUAL, 1);
   EG_DISPATCH_Q(c.q, (recovered_residual_kernel<Q><<<(total + 255) / 256, 256, 0, c.stream>>>(
                          c.geo, c.tab, c.sf, c.D, eq, er)));
+  EG_CUDA(cudaGetLastError());
+}
+
+void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x) {
+  ProfScope ps(c, EG_K_PC_APPLY, 1);
+  const long long total = (long long)nblocks * bs;
+  block_gemv_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(inv, nblocks, bs, b, x);
   EG_CUDA(cudaGetLastError());
 }
 

@@ -180,6 +180,8 @@ void launch_schur_apply(Ctx &c, const double *v, double *y);
 void launch_recover(Ctx &c, const double *lam, double *du);
 void launch_recovered_residual(Ctx &c, const double *eq, double *er);
 void launch_schur_jacobi(Ctx &c, bool factor);
+// x = Inv b for explicit block inverses (Schur block Jacobi apply).
+void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x);
 // ---- launchers (eg_krylov.cu) ----
 // Weighted squared norm sum(metric * x * x) into dscal[slot] (device).
 void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot);
