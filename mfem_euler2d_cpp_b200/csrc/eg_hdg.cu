@@ -402,6 +402,18 @@ __device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, do
                : "d"(a), "d"(b));
 }
 
+// Reciprocal of a pivot: hardware estimate refined by two Newton-Raphson
+// steps r <- r + r (1 - x r) (quadratic convergence from the ~2^-20 estimate;
+// result within one unit in the last place of 1/x).
+__device__ __forceinline__ double pivot_reciprocal(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+
 template <int Q, int WR, int WC>
 struct GjCfg {
   static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, NC = M + NR;
@@ -468,7 +480,7 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
       for (int c = 0; c < 4; ++c) w[k][c] = un[k] ? pan[buf][i][c] : 0.;
     }
     int prow[4];
-    double U[4][4], dinv[4];
+    double U[4][4], dinv[4], L[4][4];
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
       unsigned hi = 0u, lo = 0u;
@@ -507,7 +519,11 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
 #pragma unroll
       for (int k = 0; k < KR; ++k)
         if (k == kk && lane == owner) un[k] = false;
-      const double inv = __drcp_rn(pw[jj]);
+      // multipliers of the new pivot row from the panel's earlier steps
+      if (jj > 0) __syncwarp();  // order the owner's earlier lmul stores before these loads
+#pragma unroll
+      for (int cc = 0; cc < jj; ++cc) L[jj][cc] = lmul[bi][cc];
+      const double inv = pivot_reciprocal(pw[jj]);
       dinv[jj] = inv;
 #pragma unroll
       for (int c = 0; c < 4; ++c) U[jj][c] = pw[c];
@@ -523,15 +539,14 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
         }
       }
     }
-    __syncwarp();
-    // T^{-1}: lane c < 4 solves T x = e_c with the factors (L from lmul, U, 1/pivots)
+    // T^{-1}: lane c < 4 solves T x = e_c with the factors (L, U, 1/pivots)
     if (lane < 4) {
       double y[4];
 #pragma unroll
       for (int rr = 0; rr < 4; ++rr) {
         double v = rr == lane ? 1. : 0.;
 #pragma unroll
-        for (int cc = 0; cc < rr; ++cc) v -= lmul[prow[rr]][cc] * y[cc];
+        for (int cc = 0; cc < rr; ++cc) v -= L[rr][cc] * y[cc];
         y[rr] = v;
       }
 #pragma unroll
@@ -544,14 +559,12 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
 #pragma unroll
       for (int rr = 0; rr < 4; ++rr) fac[buf][rr * 4 + lane] = y[rr];
     }
-#pragma unroll
-    for (int rr = 0; rr < 4; ++rr) {
-      if (lane == rr) {
-        pivs[buf][rr] = prow[rr];
-        used[prow[rr]] = 1;
-        invp[prow[rr]] = jbase + rr;
-        pan[buf][prow[rr]][rr] -= 1.;  // A operand T_r - e_r
-      }
+    if (lane < 4) {
+      const int pr = lane == 0 ? prow[0] : lane == 1 ? prow[1] : lane == 2 ? prow[2] : prow[3];
+      pivs[buf][lane] = pr;
+      used[pr] = 1;
+      invp[pr] = jbase + lane;
+      pan[buf][pr][lane] -= 1.;  // A operand T_r - e_r
     }
     return true;
   };
