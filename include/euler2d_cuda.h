@@ -274,6 +274,31 @@ int eg_stepper_create(eg_ctx *ctx, const eg_run_opts *ro, eg_stepper **out);
 int eg_stepper_next(eg_stepper *s, eg_update_stats *st);
 void eg_stepper_destroy(eg_stepper *s);
 
+/* ------------------------------------------------- allocation-free entry */
+/* CellNorm of a body vector without any device allocation. This entry point
+ * has no counterpart in the reference.
+ *
+ * It exists for callers that may not allocate device memory from library
+ * code: applications whose device memory is owned by their own allocator or
+ * memory pool (every buffer handed out and accounted for by that pool), and
+ * deployments that fix the device-memory footprint in advance. Such a caller
+ * cannot create an eg_ctx, because a context allocates its buffers.
+ *
+ * r must point to n*m doubles of device-accessible memory laid out as the
+ * reference's body vectors (host pointers are rejected with EG_ERR_INVALID);
+ * *out receives sqrt(sum_i area * mass_i * r_i^2), the same value eg_cell_norm
+ * returns for the same vector. stream may be NULL (the default stream); the
+ * call returns after the result is on the host.
+ *
+ * Scratch: a fixed 4 KB static device array inside the library (partial sums,
+ * completion counter, metric table), held by every GPU that loads the library
+ * until the process exits. Degrees k > 8 exceed its metric table and are
+ * rejected with EG_ERR_INVALID. The first call on each device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * (concurrent streams or threads) race and must be serialised by the caller. */
+int eg_cell_norm_noalloc(const eg_desc *d, const double *r, void *stream, double *out);
+
 /* ------------------------------------------------------------ profiling */
 /* Kernel classes timed with CUDA events on the context stream when
  * profiling is on (eg_profile_enable). */

@@ -124,6 +124,7 @@ def load() -> C.CDLL:
         "eg_profile_reset": (C.c_int, [vp]),
         "eg_profile_query": (C.c_int, [vp, C.c_int, _DP, C.POINTER(C.c_longlong)]),
         "eg_launch_count": (C.c_longlong, [vp]),
+        "eg_cell_norm_noalloc": (C.c_int, [C.POINTER(Desc), C.c_void_p, C.c_void_p, _DP]),
         "eg_create": (C.c_int, [C.POINTER(Desc), C.POINTER(Opts), C.POINTER(vp)]),
         "eg_destroy": (None, [vp]),
         "eg_last_error": (C.c_char_p, [vp]),
