@@ -56,6 +56,17 @@ K_NAMES = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "reco
            "recovered_residual", "schur_jacobi", "pc_apply", "krylov", "freeze", "admissible", "vector"]
 
 
+# DRAM bytes (read + write) per cell of one launch, from one ncu capture of the
+# kernel on a 64x64 mesh of the same degree (profiles/condense_gj_q4_64x64.txt,
+# profiles/cell_gemv_q4_64x64.txt); per-launch traffic grows with the cell count.
+NCU_TRAFFIC_PER_CELL = {("condense", 4): 288.21e6 / 4096, ("schur_apply", 4): 279.9e6 / 4096}
+
+
+def traffic(name, w):
+    per = NCU_TRAFFIC_PER_CELL.get((name, w["k"]))
+    return None if per is None else per * w["nx"] * w["ny"]
+
+
 def sizes(w):
     q = w["k"] + 1
     p, n = q * q, w["nx"] * w["ny"]
@@ -375,14 +386,15 @@ def run_ours(args, world, rank, local):
             achieved = units / avg_s / 1e9
             peak = peaks["hbm_gbs"]
             roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak,
-                        "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                        "unit": "GB/s", "frac": achieved / peak, "traffic": traffic(dominant, w),
                         "algorithmic_bytes_per_launch": units, "avg_launch_ms": avg_s * 1e3,
                         "launches": nops, "peak_source": f"{peak_src} hbm_gbs"}
         else:
             fp64_peak = fp64_gemm_peak()
             achieved = units / avg_s / 1e12
-            roofline = {"kernel": dominant, "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
-                        "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+            roofline = {"kernel": dominant, "bound": "tensor", "pipe": "fp64 mma (m8n8k4)",
+                        "achieved": achieved, "peak": fp64_peak,
+                        "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic(dominant, w),
                         "algorithmic_flops_per_launch": units, "avg_launch_ms": avg_s * 1e3,
                         "launches": nops,
                         "peak_source": "measured FP64 DGEMM (torch.matmul float64 4096^3) on this GPU"}
@@ -396,7 +408,7 @@ def run_ours(args, world, rank, local):
             avg_s = ms * 1e-3 / n_op
             ach = alg[name][1] / avg_s / 1e9
             hbm_lines[name] = {"achieved_gbs": ach, "frac": ach / peaks["hbm_gbs"], "avg_launch_ms": avg_s * 1e3,
-                               "launches": n_op}
+                               "launches": n_op, "traffic": traffic(name, w)}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         times, src = run_reference_updates(w, 1)
