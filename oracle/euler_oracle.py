@@ -525,6 +525,18 @@ class Problem:
             np.add.at(blocks, self.cell_faces[:, s], -panel.reshape(self.n, t, t))
         return blocks
 
+    def schur_panels(self):
+        """All 16 panels C_s R_s X_{:,o} of every cell (FaceCoupling::Panel,
+        operators.cpp:7-26): (n, 4, 4, t, t) indexed [cell, s, o]."""
+        t = self.t
+        RX = self.restrict(self.X)                                  # (n, 4, q, 4, 4t)
+        out = np.empty((self.n, 4, 4, t, t))
+        for s in range(4):
+            full = np.einsum("ejcd,ejdk->ejck", self.C[:, s], RX[:, s]).reshape(self.n, t, 4 * t)
+            for o in range(4):
+                out[:, s, o] = full[:, :, o * t:(o + 1) * t]
+        return out
+
     def recover(self, lam):
         """du_e = -X_e lam[ids_e] - y_e (condensation.cpp:9-42, 149-163)."""
         loc = np.asarray(lam, float)[self.trace_ids()]
@@ -580,6 +592,128 @@ class Problem:
         Z = np.einsum("bai,eic->ebac", S, self.cells(u))
         W = np.outer(ws, ws)
         return np.sqrt(self.area * np.einsum("ba,ebac->c", W, (Z - V) ** 2))
+
+
+# ----------------------------------------------------------------------------
+# Block ILU(0) (src/block_ilu.cpp:10-124, partial.cpp:140-170, operators.cpp:48-74)
+# ----------------------------------------------------------------------------
+
+def solver_graph(pb: Problem, hdg: bool):
+    """Problem::SolverGraph (block_ilu.cpp:110-124): cells and their face
+    neighbours (DG) or faces sharing a cell (HDG), sorted and unique."""
+    if hdg:
+        graph = [set() for _ in range(pb.nf)]
+        for local in pb.cell_faces:
+            for i in local:
+                graph[i].update(int(j) for j in local)
+    else:
+        graph = [{e} for e in range(pb.n)]
+        for f in range(pb.nf):
+            graph[pb.face_l[f]].add(int(pb.face_r[f]))
+            graph[pb.face_r[f]].add(int(pb.face_l[f]))
+    return [sorted(g) for g in graph]
+
+
+class BlockILU0:
+    """FixedBlockILU with natural ordering (block_ilu.cpp:10-109): BSR rows
+    with sorted columns, the retained ILU(0) products per strictly-lower
+    entry, in-place factorisation with pivoted diagonal LU, and the forward
+    (unit lower) / backward (upper, diagonal LU solve) apply."""
+
+    def __init__(self, graph, block: int):
+        self.rows, self.b = len(graph), block
+        self.row, self.col, self.diag = [0], [], []
+        for i in range(self.rows):
+            for j in sorted(set(graph[i]) | {i}):
+                if j == i:
+                    self.diag.append(len(self.col))
+                self.col.append(j)
+            self.row.append(len(self.col))
+        self.updates = [[] for _ in self.col]                     # block_ilu.cpp:46-57
+        for i in range(self.rows):
+            for ik in range(self.row[i], self.diag[i]):
+                k = self.col[ik]
+                ij, kj = ik + 1, self.diag[k] + 1
+                while ij < self.row[i + 1] and kj < self.row[k + 1]:
+                    if self.col[ij] < self.col[kj]:
+                        ij += 1
+                    elif self.col[kj] < self.col[ij]:
+                        kj += 1
+                    else:
+                        self.updates[ik].append((ij, kj))
+                        ij += 1
+                        kj += 1
+        self.data = np.zeros((len(self.col), block, block))
+        self.lu = [None] * self.rows
+
+    def at(self, i: int, j: int) -> int:
+        lo, hi = self.row[i], self.row[i + 1]
+        pos = lo + int(np.searchsorted(self.col[lo:hi], j))
+        require(pos < hi and self.col[pos] == j, "Entry outside fixed BSR graph")
+        return pos
+
+    def factor(self):                                               # block_ilu.cpp:74-87
+        import scipy.linalg as sla
+        for i in range(self.rows):
+            for ik in range(self.row[i], self.diag[i]):
+                k = self.col[ik]
+                # RightSolve: X <- X A_kk^{-1} with the pivoted LU of A_kk
+                self.data[ik] = sla.lu_solve(self.lu[k], self.data[ik].T, trans=1).T
+                for target, upper in self.updates[ik]:
+                    self.data[target] -= self.data[ik] @ self.data[upper]
+            a = self.data[self.diag[i]]
+            lu, piv = sla.lu_factor(a, check_finite=False)
+            require(np.all(np.isfinite(lu)) and np.all(np.diag(lu) != 0), "Singular BSR ILU diagonal")
+            self.lu[i] = (lu, piv)
+
+    def __call__(self, b):                                          # block_ilu.cpp:88-109
+        import scipy.linalg as sla
+        B = self.b
+        w = np.array(b, float).reshape(self.rows, B)
+        for i in range(self.rows):
+            for ij in range(self.row[i], self.diag[i]):
+                w[i] -= self.data[ij] @ w[self.col[ij]]
+        for i in range(self.rows - 1, -1, -1):
+            for ij in range(self.diag[i] + 1, self.row[i + 1]):
+                w[i] -= self.data[ij] @ w[self.col[ij]]
+            w[i] = sla.lu_solve(self.lu[i], w[i])
+        return w.reshape(-1)
+
+
+def fill_dg_ilu(pb: Problem, ilu: BlockILU0, u):
+    """PartialDGOperator::FillBlocks (partial.cpp:140-170): cell blocks on the
+    diagonal, face couplings l->r (+scale jr) and r->l (-scale jl) off it."""
+    ilu.data[:] = 0.0
+    diag = pb.dg_jacobi_blocks(u)                                    # also refreshes jl, jr
+    for e in range(pb.n):
+        ilu.data[ilu.at(e, e)] = diag[e]
+    scale = (pb.dt * pb.face_len / pb.area)[:, None] * pb.tab.ew[None, :]
+    tb = pb.tab
+    for f in range(pb.nf):
+        ls = 1 if f % 2 == 0 else 3
+        rs = ls - 1
+        l, r = int(pb.face_l[f]), int(pb.face_r[f])
+        lr = np.einsum("j,ji,jl,jcd->icld", scale[f], tb.fv[ls] * tb.inv_mass[None, :], tb.fv[rs],
+                       pb._jr[f]).reshape(pb.m, pb.m)
+        rl = np.einsum("j,ji,jl,jcd->icld", -scale[f], tb.fv[rs] * tb.inv_mass[None, :], tb.fv[ls],
+                       pb._jl[f]).reshape(pb.m, pb.m)
+        ilu.data[ilu.at(l, r)] += lr
+        ilu.data[ilu.at(r, l)] += rl
+
+
+def fill_hdg_ilu(pb: Problem, ilu: BlockILU0):
+    """ElementOperator::FillBlocks on the condensed operator (operators.cpp:48-74):
+    D on the diagonal, minus every cell's panels C_s X_{s,o}."""
+    t = pb.t
+    ilu.data[:] = 0.0
+    idx = np.arange(t)
+    for f in range(pb.nf):
+        ilu.data[ilu.at(f, f)][idx, idx] = pb.D[f * t:(f + 1) * t]
+    panels = pb.schur_panels()
+    for e in range(pb.n):
+        for s in range(4):
+            for o in range(4):
+                ilu.data[ilu.at(int(pb.cell_faces[e, s]), int(pb.cell_faces[e, o]))] += -panels[e, s, o]
 
 
 # ----------------------------------------------------------------------------
@@ -689,7 +823,7 @@ def linear_solve(apply, precond_blocks, rhs, metric, linear_tol=1e-12, max_krylo
     if rn == 0.0:
         return LinearResult(np.zeros(n), np.zeros(n), 0, 0.0), pc
     if pc is None:
-        pc = BlockJacobi(precond_blocks)
+        pc = precond_blocks if callable(precond_blocks) else BlockJacobi(precond_blocks)
     x, count, res_norm, residual, rhs_norm = gmres(apply, pc, rhs, metric, linear_tol, max_krylov, restart, x0)
     rel = res_norm / rhs_norm
     require(math.isfinite(rel) and rel <= max(10 * linear_tol, 1e-12),
@@ -719,8 +853,21 @@ class UpdateRecord:
     dg_relres: float
 
 
+def _preconditioner(pb: Problem, form: str, precond: str, u):
+    """Refreshed preconditioner of the current form (linear.cpp:177-203)."""
+    if precond == "block-ilu0":
+        ilu = BlockILU0(solver_graph(pb, form == "hdg"), pb.t if form == "hdg" else pb.m)
+        if form == "hdg":
+            fill_hdg_ilu(pb, ilu)
+        else:
+            fill_dg_ilu(pb, ilu, u)
+        ilu.factor()
+        return ilu
+    return BlockJacobi(pb.schur_jacobi_blocks() if form == "hdg" else pb.dg_jacobi_blocks(u))
+
+
 def newton_update(pb: Problem, form: str, u, residual, old_norm: float, linear_tol=1e-12,
-                  max_krylov=1500, restart=20):
+                  max_krylov=1500, restart=20, precond="block-jacobi"):
     """One accepted damped Newton update (stepper.cpp:136-224).  Returns the
     accepted state, its residual and the per-update record."""
     residual_norm = pb.cell_norm(residual)
@@ -728,14 +875,14 @@ def newton_update(pb: Problem, form: str, u, residual, old_norm: float, linear_t
     target = max(10 * linear_tol * residual_norm, allowance)
     if form == "dg":
         pb.dg_refresh(u)
-        blocks = pb.dg_jacobi_blocks(u)
-        lr, _ = linear_solve(pb.dg_apply, blocks, -residual, pb.cell_metric, linear_tol, max_krylov, restart)
+        lr, _ = linear_solve(pb.dg_apply, _preconditioner(pb, form, precond, u), -residual, pb.cell_metric,
+                             linear_tol, max_krylov, restart)
         du = lr.x
         er_norm = pb.cell_norm(lr.equation_residual)
         count, lrel = lr.count, lr.residual
     else:
         _, _, rhs, _ = pb.condense(u, residual)
-        blocks = pb.schur_jacobi_blocks()
+        blocks = _preconditioner(pb, form, precond, u)
         tol = linear_tol
         valid = False
         count = 0
@@ -768,7 +915,8 @@ def newton_update(pb: Problem, form: str, u, residual, old_norm: float, linear_t
 
 
 def run(nx, ny, k, alpha_deg, form="hdg", cfl=1.0, steps=1, newton_steps=1, integrator="ssp-dirk3",
-        linear_tol=1e-12, max_krylov=1500, restart=20, safety=1.1, gamma=3.0, u0=None, tables=None):
+        linear_tol=1e-12, max_krylov=1500, restart=20, safety=1.1, gamma=3.0, u0=None, tables=None,
+        precond="block-jacobi"):
     """Run() for a fixed number of steps and Newton updates per stage
     (stepper.cpp:28-292, the `--steps N --newton-steps M --cfl C` branch).
     Returns (u, records) with one UpdateRecord per update."""
@@ -803,7 +951,7 @@ def run(nx, ny, k, alpha_deg, form="hdg", cfl=1.0, steps=1, newton_steps=1, inte
                     residual = pb.residual(u)
                 rms = phys * pb.cell_norm(residual)
                 u, residual, (damping, count, lrel, dgrel) = newton_update(
-                    pb, form, u, residual, old_norm, linear_tol, max_krylov, restart)
+                    pb, form, u, residual, old_norm, linear_tol, max_krylov, restart, precond)
                 records.append(UpdateRecord(rms, damping, count, lrel, dgrel))
             slopes[stage] = (u - base) * (1.0 / pb.dt)
         if integrator != "be":

@@ -11,6 +11,7 @@
 // against the MFEM-subset shim into oracle/_ref/libeuler_ref.so.
 #include "euler.hpp"
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 
@@ -256,5 +257,59 @@ int ref_linear_solve(void *hv, int form, const double *u, const double *rhs, dou
     *count = lr.count;
     *relres = lr.residual;
   });
+}
+
+// Block ILU(0) (FixedBlockILU, block_ilu.cpp:10-109) of the DG Jacobian at u
+// (form 0, PartialDGOperator::FillBlocks partial.cpp:140) or of the condensed
+// Schur operator of the last ref_hdg_condense (form 1, ElementOperator::
+// FillBlocks operators.cpp:48), natural ordering. Blocks are returned in the
+// BSR order of FixedBlockILU (rows ascending, columns ascending), each
+// column-major: `filled` after FillBlocks, `factored` after Factor (the
+// diagonal entries then hold the pivoted LU factors). x = ILU^{-1} b.
+// With null output pointers only *nnzb is set.
+int ref_ilu(void *hv, int form, const double *u, const double *b, double *x, double *filled,
+            double *factored, int *nnzb) {
+  return guarded([&] {
+    auto *hd = static_cast<RefHandle *>(hv);
+    auto &p = *hd->p;
+    const bool hdg = form == 1;
+    const int block = hdg ? p.t : p.m, rows = hdg ? p.nf : p.n;
+    auto graph = p.SolverGraph(hdg);
+    std::vector<std::vector<int>> pattern(rows);
+    int count = 0;
+    for (int i = 0; i < rows; ++i) {
+      pattern[i] = graph[i];
+      pattern[i].push_back(i);
+      std::sort(pattern[i].begin(), pattern[i].end());
+      pattern[i].erase(std::unique(pattern[i].begin(), pattern[i].end()), pattern[i].end());
+      count += int(pattern[i].size());
+    }
+    *nnzb = count;
+    if (!x) return;
+    FixedBlockILU ilu(graph, block, "none");
+    std::unique_ptr<ElementOperator> dg;
+    if (hdg) {
+      hd->s.op->FillBlocks(ilu);
+    } else {
+      Vector uv(const_cast<double *>(u), p.nu);
+      dg = p.PartialDG(uv);
+      dg->FillBlocks(ilu);
+    }
+    const size_t bb = size_t(block) * block;
+    auto dump = [&](double *out) {
+      size_t k = 0;
+      for (int i = 0; i < rows; ++i)
+        for (int j : pattern[i]) std::memcpy(out + bb * k++, ilu.At(i, j).GetData(), sizeof(double) * bb);
+    };
+    dump(filled);
+    ilu.Factor();
+    dump(factored);
+    Vector bv(const_cast<double *>(b), rows * block), xv(x, rows * block);
+    ilu.Mult(bv, xv);
+  });
+}
+// Switch the preconditioner of an existing handle (0 block-jacobi, 1 block-ilu0).
+void ref_set_precond(void *hv, int precond) {
+  static_cast<RefHandle *>(hv)->opt.precond = precond ? "block-ilu0" : "block-jacobi";
 }
 }

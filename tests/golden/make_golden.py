@@ -48,7 +48,8 @@ def load_ref():
     for name in ["ref_problem_free", "ref_sizes", "ref_geometry", "ref_tables", "ref_initial",
                  "ref_freeze", "ref_set_old", "ref_set_dt", "ref_residual", "ref_cell_norm",
                  "ref_admissible", "ref_dg_apply", "ref_dg_jacobi_blocks", "ref_hdg_condense",
-                 "ref_schur_apply", "ref_schur_jacobi_blocks", "ref_recover", "ref_linear_solve"]:
+                 "ref_schur_apply", "ref_schur_jacobi_blocks", "ref_recover", "ref_linear_solve",
+                 "ref_ilu", "ref_set_precond"]:
         getattr(lib, name).argtypes = None
     lib.ref_problem_free.argtypes = [C.c_void_p]
     lib.ref_sizes.argtypes = [C.c_void_p, IP]
@@ -68,6 +69,8 @@ def load_ref():
     lib.ref_schur_jacobi_blocks.argtypes = [C.c_void_p, DP]
     lib.ref_recover.argtypes = [C.c_void_p, DP, DP]
     lib.ref_linear_solve.argtypes = [C.c_void_p, C.c_int, DP, DP, DP, DP, IP, DP]
+    lib.ref_ilu.argtypes = [C.c_void_p, C.c_int, DP, DP, DP, DP, DP, IP]
+    lib.ref_set_precond.argtypes = [C.c_void_p, C.c_int]
     return lib
 
 
@@ -161,6 +164,36 @@ def make_unit(lib, nx, ny, k, alpha, dense, rng):
             out[f"solve_{tag}_x"] = xs
             out[f"solve_{tag}_count"] = cnt
             out[f"solve_{tag}_relres"] = rel
+        # block ILU(0) of both forms: the preconditioner apply on a seeded
+        # vector, the filled and factored BSR blocks on the small cases, and
+        # one GMRES solve per form with block-ilu0 (block_ilu.cpp, linear.cpp)
+        irng = np.random.default_rng([20261204, nx, ny, k])  # own stream: other draws unchanged
+        for form, (tag, B, rows) in {0: ("dg", m, n), 1: ("hdg", t, nf)}.items():
+            nz = np.zeros(1, np.int32)
+            check(lib, lib.ref_ilu(h, form, ptr(u), None, None, None, None, nz.ctypes.data_as(IP)))
+            nnzb = int(nz[0])
+            bvec = irng.standard_normal(rows * B)
+            xv = np.zeros(rows * B)
+            filled, factored = np.zeros(nnzb * B * B), np.zeros(nnzb * B * B)
+            check(lib, lib.ref_ilu(h, form, ptr(u), ptr(bvec), ptr(xv), ptr(filled), ptr(factored),
+                                   nz.ctypes.data_as(IP)))
+            out[f"ilu_{tag}_b"] = bvec
+            out[f"ilu_{tag}_x"] = xv
+            if (form == 0 and k <= 2) or (form == 1 and dense and k <= 3):
+                out[f"ilu_{tag}_filled"] = filled
+                out[f"ilu_{tag}_factored"] = factored
+        lib.ref_set_precond(h, 1)
+        for form, (rhs_f, N) in {0: (-r, nu), 1: (rhs, nl)}.items():
+            rr = np.ascontiguousarray(rhs_f)
+            xs, eq = np.zeros(N), np.zeros(N)
+            cnt, rel = np.zeros(1, np.int32), np.zeros(1)
+            check(lib, lib.ref_linear_solve(h, form, ptr(u), ptr(rr), ptr(xs), ptr(eq),
+                                            cnt.ctypes.data_as(IP), ptr(rel)))
+            tag = "dg" if form == 0 else "hdg"
+            out[f"solve_{tag}_ilu_x"] = xs
+            out[f"solve_{tag}_ilu_count"] = cnt
+            out[f"solve_{tag}_ilu_relres"] = rel
+        lib.ref_set_precond(h, 0)
         return out
     finally:
         lib.ref_problem_free(h)
@@ -184,6 +217,8 @@ CLI_CASES = {
                    "--steps", "1", "--newton-steps", "1", "--integrator", "be", "--form", "both"],
     "smoke_8x8_q1": ["--nx", "8", "--ny", "8", "--k", "1", "--cfl", ".1", "--steps", "1",
                      "--form", "both", "--newton-tol", "1e-12", "--linear-tol", "1e-12"],
+    "ilu_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "30", "--cfl", "1", "--steps", "1",
+                   "--newton-steps", "2", "--form", "both", "--precond", "block-ilu0"],
     "be_converged_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--cfl", ".1", "--steps", "1",
                             "--integrator", "be", "--form", "both", "--check-update",
                             "--newton-tol", "1e-12", "--linear-tol", "1e-12"],

@@ -121,11 +121,12 @@ def _cli_case(name):
     opt = lambda flag, default: type(default)(args[args.index(flag) + 1]) if flag in args else default
     kw = dict(nx=opt("--nx", 100), ny=opt("--ny", 100), k=opt("--k", 1), alpha_deg=opt("--alpha-deg", 45.0),
               cfl=opt("--cfl", -1.0), steps=opt("--steps", -1), newton_steps=opt("--newton-steps", -1),
-              integrator=opt("--integrator", "ssp-dirk3"), linear_tol=opt("--linear-tol", 1e-12))
+              integrator=opt("--integrator", "ssp-dirk3"), linear_tol=opt("--linear-tol", 1e-12),
+              precond=opt("--precond", "block-jacobi"))
     return f, kw
 
 
-@pytest.mark.parametrize("name", ["be1_8x8_q2", "c1_16x16_q3"])
+@pytest.mark.parametrize("name", ["be1_8x8_q2", "c1_16x16_q3", "ilu_8x8_q2"])
 @pytest.mark.parametrize("form", ["dg", "hdg"])
 def test_time_loop_matches_reference_cli(name, form):
     f, kw = _cli_case(name)
@@ -166,3 +167,46 @@ def test_oracle_errors_carry_reference_messages():
     pb2.dg_refresh(u2)
     with pytest.raises(eo.OracleError, match="GMRES iteration limit reached"):
         eo.linear_solve(pb2.dg_apply, pb2.dg_jacobi_blocks(u2), -r, pb2.cell_metric, 1e-12, 2, 20)
+
+
+def _ilu_of(pb, f, hdg):
+    ilu = eo.BlockILU0(eo.solver_graph(pb, hdg), pb.t if hdg else pb.m)
+    if hdg:
+        pb.condense(f["u"], f["r"])
+        eo.fill_hdg_ilu(pb, ilu)
+    else:
+        eo.fill_dg_ilu(pb, ilu, f["u"])
+    return ilu
+
+
+@pytest.mark.parametrize("path", unit_files(), ids=lambda p: p.stem)
+@pytest.mark.parametrize("tag", ["dg", "hdg"])
+def test_block_ilu0_fill_factor_apply(path, tag):
+    f = np.load(path)
+    pb = _problem(f)
+    hdg = tag == "hdg"
+    ilu = _ilu_of(pb, f, hdg)
+    B = ilu.b
+    nnzb = len(ilu.col)
+    if f"ilu_{tag}_filled" in f.files:
+        ref = _colmajor(f[f"ilu_{tag}_filled"], nnzb, B, B)
+        assert rel_err(ilu.data, ref) < 1e-11
+    ilu.factor()
+    if f"ilu_{tag}_factored" in f.files:
+        ref = _colmajor(f[f"ilu_{tag}_factored"], nnzb, B, B)
+        off = np.ones(nnzb, bool)
+        off[ilu.diag] = False
+        assert rel_err(ilu.data[off], ref[off]) < 1e-10
+        # diagonal entries hold the row-pivoted LU factors (LAPACK packing)
+        packed = np.stack([ilu.lu[i][0] for i in range(ilu.rows)])
+        assert rel_err(packed, ref[ilu.diag]) < 1e-10
+    assert rel_err(ilu(f[f"ilu_{tag}_b"]), f[f"ilu_{tag}_x"]) < 1e-10
+    # one weighted GMRES solve preconditioned by the ILU
+    if hdg:
+        rhs, apply, metric = pb.condense(f["u"], f["r"])[2], pb.schur_apply, pb.trace_metric
+    else:
+        pb.dg_refresh(f["u"])
+        rhs, apply, metric = -np.asarray(f["r"]), pb.dg_apply, pb.cell_metric
+    lr, _ = eo.linear_solve(apply, ilu, rhs, metric, 1e-12, 1500, 20)
+    assert rel_err(lr.x, f[f"solve_{tag}_ilu_x"]) < SOLVE_TOL
+    assert abs(lr.count - int(f[f"solve_{tag}_ilu_count"][0])) <= 1
