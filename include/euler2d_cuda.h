@@ -58,7 +58,9 @@ enum eg_status {
   EG_ERR_INITIAL = 21,          /* "Initial projection not positive; refine mesh" stepper.cpp:32 */
   EG_ERR_UPDATE_EQUATION = 22,  /* "Independent recovered DG equation check failed" stepper.cpp:190 */
   EG_ERR_UPDATE_EQUIVALENCE = 23, /* "DG/HDG one-update equivalence failed" stepper.cpp:197 */
-  EG_ERR_COUNT = 24
+  EG_ERR_WAIT_LIMIT = 24,       /* a bounded device-side wait of a dependency-driven sweep gave up
+                                   (no counterpart in the reference, which runs the sweep serially) */
+  EG_ERR_COUNT = 25
 };
 
 enum eg_form { EG_FORM_DG = 0, EG_FORM_HDG = 1 };
@@ -80,8 +82,12 @@ enum eg_slot {
   EG_SLOT_D = 6,       /* HDG trace diagonal D (nl) */
   EG_SLOT_X = 7,       /* HDG responses X, n blocks of m x 4t column-major */
   EG_SLOT_Y = 8,       /* HDG particular responses y (nu) */
-  EG_SLOT_PC_BLOCKS = 9, /* preconditioner blocks (DG: n*m*m, HDG: nf*t*t), column-major;
-                          after eg_pc_factor(ctx, 1): DG packed pivoted LU, HDG explicit inverse */
+  EG_SLOT_PC_BLOCKS = 9, /* preconditioner blocks, column-major (count: eg_pc_size).
+                          block-jacobi: DG n*m*m, HDG nf*t*t; after eg_pc_factor(ctx, 1) DG
+                          holds packed pivoted LU, HDG explicit inverses.
+                          block-ilu0: the BSR blocks of the ILU in FixedBlockILU order (rows
+                          ascending, block columns ascending); after eg_pc_factor(ctx, 1) the
+                          strictly lower blocks hold L, the others U (diagonal unfactored). */
   EG_SLOT_HLL_A = 10,  /* frozen left HLL bound per face point (nf*q) */
   EG_SLOT_HLL_B = 11,  /* frozen right HLL bound per face point (nf*q) */
   EG_SLOT_COUNT = 12
@@ -207,7 +213,11 @@ int eg_recover(eg_ctx *ctx, const double *lam, double *du);
  * (src/linear.cpp:186-203): DiagonalBlocks+LU or FillBlocks+ILU factor for the
  * current form. factor=0 stops after building (for EG_SLOT_PC_BLOCKS parity). */
 int eg_pc_factor(eg_ctx *ctx, int factor);
-/* Replaces: LinearSolver::Impl::Precondition (src/linear.cpp:66). */
+/* Number of doubles in EG_SLOT_PC_BLOCKS for the current form and
+ * preconditioner (0 before the first eg_pc_factor with block-ilu0). */
+int eg_pc_size(const eg_ctx *ctx, long long *count);
+/* Replaces: LinearSolver::Impl::Precondition (src/linear.cpp:66) with block
+ * Jacobi, FixedBlockILU::Mult (src/block_ilu.cpp:88) with block-ilu0. */
 int eg_pc_apply(eg_ctx *ctx, const double *b, double *x);
 /* Replaces: LinearSolver::Solve (src/linear.cpp:167) for the current form:
  * weighted right-preconditioned restarted CGS2 GMRES. x is in/out (used as

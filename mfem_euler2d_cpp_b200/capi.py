@@ -30,7 +30,7 @@ STATUS_NAMES = {
     13: "EG_ERR_LINEAR_RESIDUAL", 14: "EG_ERR_RECOVERED", 15: "EG_ERR_DG_LINEAR",
     16: "EG_ERR_LINE_SEARCH", 17: "EG_ERR_OUT_OF_MEMORY", 18: "EG_ERR_STEP_INTERVAL",
     19: "EG_ERR_NEWTON_CONVERGE", 20: "EG_ERR_DIRK_INADMISSIBLE", 21: "EG_ERR_INITIAL",
-    22: "EG_ERR_UPDATE_EQUATION", 23: "EG_ERR_UPDATE_EQUIVALENCE",
+    22: "EG_ERR_UPDATE_EQUATION", 23: "EG_ERR_UPDATE_EQUIVALENCE", 24: "EG_ERR_WAIT_LIMIT",
 }
 FORM_DG, FORM_HDG = 0, 1
 PC_JACOBI, PC_ILU0 = 0, 1
@@ -147,6 +147,7 @@ def load() -> C.CDLL:
         "eg_recover": (C.c_int, [vp, _DP, _DP]),
         "eg_pc_factor": (C.c_int, [vp, C.c_int]),
         "eg_pc_apply": (C.c_int, [vp, _DP, _DP]),
+        "eg_pc_size": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "eg_linear_solve": (C.c_int, [vp, _DP, _DP, _DP, C.c_int, C.c_double,
                                       C.POINTER(LinearStats)]),
         "eg_stage_begin": (C.c_int, [vp, C.c_double]),
@@ -232,8 +233,7 @@ class Context:
         return {"U": self.nu, "OLD": self.nu, "R": self.nu, "DU": self.nu, "RHS": self.nl,
                 "LAMBDA": self.nl, "D": self.nl, "X": self.n * self.m * 4 * self.t, "Y": self.nu,
                 "HLL_A": self.nf * self.q, "HLL_B": self.nf * self.q,
-                "PC_BLOCKS": (self.n * self.m * self.m if self.opts.form == FORM_DG
-                              else self.nf * self.t * self.t)}[slot]
+                "PC_BLOCKS": self.pc_size()}[slot]
 
     def upload(self, slot: str, x: np.ndarray):
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -289,6 +289,11 @@ class Context:
         du = np.empty(self.nu)
         self._check(self.lib.eg_recover(self.h, _ptr(lam), _ptr(du)))
         return du
+
+    def pc_size(self) -> int:
+        count = C.c_longlong()
+        self._check(self.lib.eg_pc_size(self.h, C.byref(count)))
+        return count.value
 
     def pc_factor(self, factor: bool = True):
         self._check(self.lib.eg_pc_factor(self.h, int(factor)))

@@ -49,6 +49,7 @@ static const char *kMessages[EG_ERR_COUNT] = {
     "Initial projection not positive; refine mesh",
     "Independent recovered DG equation check failed",
     "DG/HDG one-update equivalence failed",
+    "device wait limit reached",
 };
 
 void *Ctx::alloc(size_t nbytes) {
@@ -169,7 +170,10 @@ struct DgOps : LinearOps {
   }
   void apply(Ctx &c, const double *x, double *y) override { launch_dg_apply(c, c.u, x, y); }
   void precondition(Ctx &c, const double *b, double *x) override {
-    launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, b, x);
+    if (c.opts.precond == EG_PC_BLOCK_ILU0)
+      launch_ilu_apply(c, EG_FORM_DG, b, x);
+    else
+      launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, b, x);
   }
 };
 struct HdgOps : LinearOps {
@@ -180,14 +184,18 @@ struct HdgOps : LinearOps {
   }
   void apply(Ctx &c, const double *x, double *y) override { launch_schur_apply(c, x, y); }
   void precondition(Ctx &c, const double *b, double *x) override {
-    launch_block_inverse_apply(c, c.pc_hdg, c.nf, c.t, b, x);
+    if (c.opts.precond == EG_PC_BLOCK_ILU0)
+      launch_ilu_apply(c, EG_FORM_HDG, b, x);
+    else
+      launch_block_inverse_apply(c, c.pc_hdg, c.nf, c.t, b, x);
   }
 };
 
 static void pc_factor(Ctx &c, int form, bool factor) {
-  if (c.opts.precond != EG_PC_BLOCK_JACOBI)
-    fail(EG_ERR_INVALID, "block-ilu0 is not available in this build");
-  if (form == EG_FORM_DG) {
+  if (c.opts.precond == EG_PC_BLOCK_ILU0) {
+    // FillBlocks + FixedBlockILU::Factor (src/linear.cpp:191, 196-197)
+    ilu_refresh(c, form, factor);
+  } else if (form == EG_FORM_DG) {
     launch_dg_jacobi(c, c.u, factor);
   } else {
     if (!c.condensed) fail(EG_ERR_INVALID, "Schur preconditioner requires a condensation");
@@ -222,7 +230,14 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
   out.setup = now_s() - t0;
   t0 = now_s();
   int count = 0;
-  const double res = gmres(c, ops, rhs, x, tol, c.opts.max_krylov, refresh, &count, nullptr);
+  double res = 0.;
+  try {
+    res = gmres(c, ops, rhs, x, tol, c.opts.max_krylov, refresh, &count, nullptr);
+  } catch (const Failure &) {
+    c.check_device_error();  // a preconditioner failure on the device explains the breakdown
+    throw;
+  }
+  c.check_device_error();
   out.solve = now_s() - t0;
   out.count = count;
   if (eq) launch_axpby(c, ops.N, -1., c.kres, 0., c.kres, eq);
@@ -602,6 +617,12 @@ int eg_download(eg_ctx *ctx, int slot, double *dst) {
       c.sync();
       return;
     }
+    if (slot == EG_SLOT_PC_BLOCKS && c.opts.precond == EG_PC_BLOCK_ILU0) {
+      const eg::IluPlan &P = c.ilu[c.opts.form];
+      if (!P.built) eg::fail(EG_ERR_INVALID, "no preconditioner built");
+      eg::download_vec(c, dst, P.data, (size_t)P.nnzb * P.B * P.B);
+      return;
+    }
     if (slot == EG_SLOT_PC_BLOCKS) {
       if (c.opts.form == EG_FORM_DG) {
         if (!c.pc_dg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
@@ -736,19 +757,41 @@ int eg_pc_factor(eg_ctx *ctx, int factor) {
   return guard(ctx, [&] { eg::pc_factor(ctx->c, ctx->c.opts.form, factor != 0); });
 }
 
+int eg_pc_size(const eg_ctx *ctx, long long *count) {
+  if (!ctx || !count) return EG_ERR_INVALID;
+  const Ctx &c = ctx->c;
+  if (c.opts.precond == EG_PC_BLOCK_ILU0) {
+    const eg::IluPlan &P = c.ilu[c.opts.form];
+    *count = P.built ? (long long)P.nnzb * P.B * P.B : 0;
+  } else {
+    *count = c.opts.form == EG_FORM_DG ? (long long)c.n * c.m * c.m : (long long)c.nf * c.t * c.t;
+  }
+  return EG_OK;
+}
+
 int eg_pc_apply(eg_ctx *ctx, const double *b, double *x) {
   if (!ctx) return EG_ERR_INVALID;
   return guard(ctx, [&] {
     Ctx &c = ctx->c;
+    const bool ilu = c.opts.precond == EG_PC_BLOCK_ILU0;
     if (c.opts.form == EG_FORM_DG) {
-      if (!c.pc_dg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
+      if (ilu ? !c.ilu[EG_FORM_DG].built : !c.pc_dg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
       eg::upload_vec(c, c.tmp_body, b, c.nu);
-      eg::launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, c.tmp_body, c.er);
+      if (ilu)
+        eg::launch_ilu_apply(c, EG_FORM_DG, c.tmp_body, c.er);
+      else
+        eg::launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, c.tmp_body, c.er);
+      c.check_device_error();
       eg::download_vec(c, x, c.er, c.nu);
     } else {
-      if (!c.pc_hdg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
+      if (ilu ? !c.ilu[EG_FORM_HDG].built : !c.pc_hdg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
+      c.ensure_hdg();
       eg::upload_vec(c, c.tmp_trace, b, c.nl);
-      eg::launch_block_inverse_apply(c, c.pc_hdg, c.nf, c.t, c.tmp_trace, c.lam);
+      if (ilu)
+        eg::launch_ilu_apply(c, EG_FORM_HDG, c.tmp_trace, c.lam);
+      else
+        eg::launch_block_inverse_apply(c, c.pc_hdg, c.nf, c.t, c.tmp_trace, c.lam);
+      c.check_device_error();
       eg::download_vec(c, x, c.lam, c.nl);
     }
   });

@@ -247,24 +247,7 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     cell_traces<Q>(st, us, UT);
     __syncthreads();
-    // DG face matrices: own-left sides add lw J(U_L) + pen I, own-right sides
-    // subtract rw J(U_R) - pen I (src/partial.cpp:272-294).
-    for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
-      const int s = task / Q, j = task % Q;
-      const bool L = side_is_left(s);
-      const int f = cell_face(e, s, g.nx, g.ny);
-      const int fi = f * Q + j;
-      double jm[16];
-      jacobian(UT + 4 * task, s < 2 ? 0 : 1, g.gm1, jm);
-      const double wgt = L ? fz.lw[fi] : fz.rw[fi], pen = fz.pen[fi];
-      double *fm = FM + task * 16;
-#pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const bool diag = (k % 5) == 0;
-        const double v = wgt * jm[k] + (diag ? (L ? pen : -pen) : 0.);
-        fm[k] = L ? v : -v;
-      }
-    }
+    dg_face_matrices<Q>(UT, FM, g, fz, e);
     __syncthreads();
     double *A = SM ? dyn : blocks + (size_t)e * M * M;
     build_cell_matrix<Q>(A, M, st, us, FM, g);

@@ -61,6 +61,29 @@ __device__ void build_cell_matrix(double *A, int lda, const STab<Q> &st, const d
   }
 }
 
+// Signed DG face matrices of cell e from its traces UT: own-left sides add
+// lw J(U_L) + pen I, own-right sides subtract rw J(U_R) - pen I
+// (src/partial.cpp:272-294); FM[(s*Q+j)*16 + c + 4d].
+template <int Q>
+__device__ void dg_face_matrices(const double *UT, double *FM, const Geo &g, const Frozen &fz, int e) {
+  for (int task = threadIdx.x; task < 4 * Q; task += blockDim.x) {
+    const int s = task / Q, j = task % Q;
+    const bool L = side_is_left(s);
+    const int f = cell_face(e, s, g.nx, g.ny);
+    const int fi = f * Q + j;
+    double jm[16];
+    jacobian(UT + 4 * task, s < 2 ? 0 : 1, g.gm1, jm);
+    const double wgt = L ? fz.lw[fi] : fz.rw[fi], pen = fz.pen[fi];
+    double *fm = FM + task * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const bool diag = (k % 5) == 0;
+      const double v = wgt * jm[k] + (diag ? (L ? pen : -pen) : 0.);
+      fm[k] = L ? v : -v;
+    }
+  }
+}
+
 // Own traces of the cell at all 4Q face points into UT[(s*Q+j)*4 + c].
 template <int Q>
 __device__ void cell_traces(const STab<Q> &st, const double *us, double *UT) {

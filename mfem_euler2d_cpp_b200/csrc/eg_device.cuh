@@ -56,7 +56,7 @@ __device__ __forceinline__ int line_node(int s, int j, int l) {
 }
 
 // Periodic neighbours; sides 0=x-, 1=x+, 2=y-, 3=y+ (src/problem.cpp:150-156).
-__device__ __forceinline__ int neighbour(int e, int s, int nx, int ny) {
+__host__ __device__ __forceinline__ int neighbour(int e, int s, int nx, int ny) {
   const int ix = e % nx, iy = e / nx;
   switch (s) {
     case 0: return iy * nx + (ix == 0 ? nx - 1 : ix - 1);
@@ -66,7 +66,7 @@ __device__ __forceinline__ int neighbour(int e, int s, int nx, int ny) {
   }
 }
 // Face of cell e on side s; the cell is the face's left cell on sides 1 and 3.
-__device__ __forceinline__ int cell_face(int e, int s, int nx, int ny) {
+__host__ __device__ __forceinline__ int cell_face(int e, int s, int nx, int ny) {
   if (s == 1) return 2 * e;
   if (s == 3) return 2 * e + 1;
   return 2 * neighbour(e, s, nx, ny) + (s == 2 ? 1 : 0);
@@ -150,6 +150,7 @@ enum DevErr : int {
   DERR_SINGULAR_CELL = 7,
   DERR_SINGULAR_JACOBI = 8,
   DERR_SINGULAR_ILU = 9,
+  DERR_WAIT_LIMIT = 24,
 };
 __device__ __forceinline__ void raise_err(int *err, int code) { atomicCAS(err, 0, code); }
 

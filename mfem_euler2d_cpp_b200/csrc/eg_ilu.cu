@@ -1,0 +1,741 @@
+// Block ILU(0) preconditioner on the DG cell graph or the condensed HDG face
+// graph, natural ordering (FixedBlockILU, src/block_ilu.cpp:10-109;
+// Problem::SolverGraph, src/block_ilu.cpp:110-124).
+//
+// Structure (host, once per context and form): BSR rows in natural order with
+// sorted block columns, the diagonal entry of each row, and for every
+// strictly lower entry (i,k) the (target i,j ; upper k,j) products that ILU(0)
+// retains (block_ilu.cpp:46-57).
+//
+// Numeric fill (every refresh): DG blocks are the cell Jacobian blocks and the
+// face couplings of PartialDGOperator::FillBlocks (src/partial.cpp:140-170);
+// HDG blocks are D - sum over cells of the panels C_s X_{s,o}
+// (ElementOperator::FillBlocks, src/operators.cpp:48-74), summed in cell order.
+//
+// Factor and apply are dependency-driven sweeps, one cooperative launch each.
+// Rows are grouped in chunks of one grid row (2nx faces or nx cells); chunk c
+// belongs to CTA c mod G, and every CTA walks its rows in increasing
+// (forward, factor) or decreasing (backward) order. A CTA publishes how many
+// of its rows are final in one 64-bit counter tagged with the launch's epoch;
+// a row waits only for rows earlier in the sweep order, which co-resident
+// CTAs own, so no wait can depend on itself. Every wait is bounded: on
+// timeout the kernel records DERR_WAIT_LIMIT, sets the abort word, and all
+// CTAs leave at their next wait (after their own bulk copies have landed).
+//
+// The factor stores the explicit inverse of each factored diagonal block
+// (pivoted LU applied to the identity), so RightSolve becomes a product with
+// it and the backward solve a block GEMV; the arithmetic is the reference's up
+// to rounding.
+#include <algorithm>
+#include <vector>
+
+#include "eg_cellmat.cuh"
+#include "eg_internal.h"
+
+namespace eg {
+namespace {
+
+constexpr unsigned kSpinLimit = 1u << 24;  // polls per wait, each with a short sleep
+constexpr unsigned kCopySpinLimit = 1u << 16;  // try_wait itself suspends between polls
+constexpr int kStageBlocks = 4;             // blocks staged per warp and row
+constexpr int kStageMaxB = 36;              // larger blocks are read from global memory
+constexpr size_t kSweepSmemBudget = 200 * 1024;
+
+// ------------------------------------------------------------ sync helpers
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
+
+__device__ __forceinline__ void give_up(int *abort, int *err) {
+  atomicExch(abort, 1);
+  raise_err(err, DERR_WAIT_LIMIT);
+}
+// Bounded wait until *p >= target (another CTA's progress).
+__device__ bool wait_progress(const unsigned long long *p, unsigned long long target, int *abort, int *err) {
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    if (ld_acquire(p) >= target) return true;
+    if (ld_volatile(abort)) return false;
+    if (it >= 16) __nanosleep(64);
+  }
+  give_up(abort, err);
+  return false;
+}
+// Bounded wait until the CTA's own published row count reaches target.
+__device__ bool wait_local(const volatile unsigned *count, unsigned target, int *abort, int *err) {
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    if (*count >= target) return true;
+    if (ld_volatile(abort)) return false;
+    if (it >= 16) __nanosleep(32);
+  }
+  give_up(abort, err);
+  return false;
+}
+
+// mbarrier + bulk copy (TMA, no multicast) into this CTA's shared memory.
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (unsigned it = 0; it < kCopySpinLimit; ++it)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+// ------------------------------------------------------------- scheduling
+struct Sched {
+  int chunk, chunks, G;
+};
+__device__ __forceinline__ int owned_chunks(const Sched &s, int g) { return (s.chunks - g + s.G - 1) / s.G; }
+template <bool BACK>
+__device__ __forceinline__ int slot_row(const Sched &s, int g, int K, int slot) {
+  const int k = slot / s.chunk, o = slot % s.chunk;
+  if (!BACK) return (g + k * s.G) * s.chunk + o;
+  return (g + (K - 1 - k) * s.G) * s.chunk + (s.chunk - 1 - o);
+}
+template <bool BACK>
+__device__ __forceinline__ void row_owner(const Sched &s, int j, int &owner, int &slot) {
+  const int c = j / s.chunk, o = j % s.chunk, k = c / s.G;
+  owner = c % s.G;
+  if (!BACK) {
+    slot = k * s.chunk + o;
+  } else {
+    const int K = owned_chunks(s, owner);
+    slot = (K - 1 - k) * s.chunk + (s.chunk - 1 - o);
+  }
+}
+
+// ------------------------------------------------------------ sweep kernel
+struct SweepArgs {
+  Sched sc;
+  int B;
+  const int *row, *col, *diag;
+  const double *data, *dinv;
+  const double *in;  // forward: b; backward: the forward result w
+  double *out;       // forward: w; backward: x
+  unsigned long long *progress;
+  int *abort, *err;
+  unsigned long long tag;
+  int staged;        // stage up to kStageBlocks blocks per row in shared memory
+};
+
+// FixedBlockILU::Mult (src/block_ilu.cpp:88-109). Forward: w_i = b_i -
+// sum_{j<i} L_ij w_j. Backward: x_i = U_ii^{-1} (w_i - sum_{j>i} U_ij x_j).
+// One warp per row, lanes own block rows r = lane + 32 s; W warps per CTA keep
+// W rows (and their block copies) in flight; rows are published in order.
+template <int S, bool BACK>
+__global__ void __launch_bounds__(256) ilu_sweep_kernel(SweepArgs a) {
+  extern __shared__ __align__(128) double smem[];
+  __shared__ unsigned done_local;
+  __shared__ __align__(8) unsigned long long bars[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const int g = blockIdx.x, B = a.B;
+  const size_t BB = (size_t)B * B;
+  const int K = owned_chunks(a.sc, g), nslots = K * a.sc.chunk;
+  const size_t stage_doubles = a.staged ? kStageBlocks * BB : 0;
+  double *stage = smem + (size_t)warp * stage_doubles;
+  double *vb = smem + (size_t)W * stage_doubles + (size_t)warp * 32 * S;
+  if (threadIdx.x == 0) done_local = 0;
+  if (a.staged && lane == 0) mbar_init(&bars[warp]);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
+  volatile unsigned *dl = &done_local;
+  unsigned phase = 0;
+  for (int slot = warp; slot < nslots; slot += W) {
+    const int i = slot_row<BACK>(a.sc, g, K, slot);
+    const int e0 = BACK ? a.diag[i] + 1 : a.row[i];
+    const int e1 = BACK ? a.row[i + 1] : a.diag[i];
+    const int ne = e1 - e0;
+    const int nst = a.staged ? min(ne, BACK ? kStageBlocks - 1 : kStageBlocks) : 0;
+    const bool copy = a.staged && (nst > 0 || BACK);
+    if (copy && lane == 0) {
+      const unsigned bytes = (unsigned)(sizeof(double) * BB * (nst + (BACK ? 1 : 0)));
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect(&bars[warp], bytes);
+      if (nst) bulk_load(stage, a.data + (size_t)e0 * BB, (unsigned)(sizeof(double) * BB * nst), &bars[warp]);
+      if (BACK) bulk_load(stage + (size_t)nst * BB, a.dinv + (size_t)i * BB, (unsigned)(sizeof(double) * BB),
+                          &bars[warp]);
+    }
+    double acc[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int r = lane + 32 * s;
+      acc[s] = r < B ? __ldcg(a.in + (size_t)i * B + r) : 0.;
+    }
+    if (copy) {
+      if (!mbar_wait(&bars[warp], phase)) {
+        give_up(a.abort, a.err);
+        mbar_wait(&bars[warp], phase);  // let the copy land before the CTA can exit
+        return;
+      }
+      phase ^= 1u;
+    }
+    bool ok = true;
+    for (int e = e0; e < e1; ++e) {
+      const int j = a.col[e];
+      int owner, js;
+      row_owner<BACK>(a.sc, j, owner, js);
+      ok = owner == g ? wait_local(dl, (unsigned)js + 1, a.abort, a.err)
+                      : wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
+      if (!ok) break;
+      __threadfence_block();
+      for (int r = lane; r < B; r += 32) vb[r] = __ldcg(a.out + (size_t)j * B + r);
+      __syncwarp();
+      const double *A = e - e0 < nst ? stage + (size_t)(e - e0) * BB : a.data + (size_t)e * BB;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int r = lane + 32 * s;
+        if (r < B) {
+          double t = acc[s];
+          for (int cc = 0; cc < B; ++cc) t -= A[(size_t)cc * B + r] * vb[cc];
+          acc[s] = t;
+        }
+      }
+      __syncwarp();
+    }
+    if (!ok) return;
+    if (BACK) {
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int r = lane + 32 * s;
+        if (r < B) vb[r] = acc[s];
+      }
+      __syncwarp();
+      const double *Di = a.staged ? stage + (size_t)nst * BB : a.dinv + (size_t)i * BB;
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int r = lane + 32 * s;
+        if (r < B) {
+          double t = 0.;
+          for (int cc = 0; cc < B; ++cc) t += Di[(size_t)cc * B + r] * vb[cc];
+          acc[s] = t;
+        }
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int r = lane + 32 * s;
+      if (r < B) a.out[(size_t)i * B + r] = acc[s];
+    }
+    __threadfence();
+    __syncwarp();
+    int pub = 1;
+    if (lane == 0) {
+      pub = wait_local(dl, (unsigned)slot, a.abort, a.err);  // rows are published in order
+      if (pub) {
+        *dl = (unsigned)slot + 1;
+        st_release(a.progress + g, a.tag | (unsigned long long)(slot + 1));
+      }
+    }
+    if (!__shfl_sync(0xffffffffu, pub, 0)) return;
+  }
+}
+
+// ----------------------------------------------------------- factor kernel
+struct FactorArgs {
+  Sched sc;
+  int B;
+  const int *row, *col, *diag, *upd_ptr, *upd;
+  double *data, *dinv, *work;
+  unsigned long long *progress;
+  int *abort, *err;
+  unsigned long long tag;
+};
+
+// FixedBlockILU::Factor (src/block_ilu.cpp:74-87), one CTA per row: for each
+// lower entry (i,k) in column order, L_ik = A_ik U_kk^{-1}, then A_ij -= L_ik
+// U_kj over the retained products; finally the pivoted LU of the diagonal
+// block, stored as its explicit inverse.
+template <int RMAX, bool SMEM>
+__global__ void __launch_bounds__(256) ilu_factor_kernel(FactorArgs a) {
+  extern __shared__ __align__(16) double fsm[];
+  __shared__ int piv_s[32 * RMAX];
+  __shared__ double inv_piv[32 * RMAX];
+  __shared__ double bcast[2];
+  __shared__ int stop;
+  const int B = a.B;
+  const int BB = B * B;
+  const int g = blockIdx.x, K = owned_chunks(a.sc, g), nslots = K * a.sc.chunk;
+  double *Lt = SMEM ? fsm : a.work + (size_t)g * 3 * BB;
+  double *Sd = Lt + BB, *Inv = Sd + BB;
+  for (int slot = 0; slot < nslots; ++slot) {
+    const int i = slot_row<false>(a.sc, g, K, slot);
+    if (threadIdx.x == 0) {
+      int ok = 1;
+      for (int e = a.row[i]; e < a.diag[i] && ok; ++e) {
+        int owner, js;
+        row_owner<false>(a.sc, a.col[e], owner, js);
+        if (owner != g) ok = wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
+      }
+      stop = !ok;
+    }
+    __syncthreads();
+    if (stop) return;
+    for (int ik = a.row[i]; ik < a.diag[i]; ++ik) {
+      const int k = a.col[ik];
+      double *Aik = a.data + (size_t)ik * BB;
+      const double *Dk = a.dinv + (size_t)k * BB;
+      for (int o = threadIdx.x; o < BB; o += blockDim.x) {
+        const int r = o % B, cc = o / B;
+        double sum = 0.;
+        for (int s = 0; s < B; ++s) sum += Aik[(size_t)s * B + r] * __ldcg(Dk + (size_t)cc * B + s);
+        Lt[o] = sum;
+      }
+      __syncthreads();
+      for (int o = threadIdx.x; o < BB; o += blockDim.x) Aik[o] = Lt[o];
+      const int u0 = a.upd_ptr[ik], nu = a.upd_ptr[ik + 1] - u0;
+      for (int t = threadIdx.x; t < nu * BB; t += blockDim.x) {
+        const int uu = u0 + t / BB, o = t % BB;
+        const int r = o % B, cc = o / B;
+        double *T = a.data + (size_t)a.upd[2 * uu] * BB;
+        const double *U = a.data + (size_t)a.upd[2 * uu + 1] * BB;
+        double sum = 0.;
+        for (int s = 0; s < B; ++s) sum += Lt[(size_t)s * B + r] * __ldcg(U + (size_t)cc * B + s);
+        T[o] -= sum;
+      }
+      __syncthreads();
+    }
+    const double *Ad = a.data + (size_t)a.diag[i] * BB;
+    for (int o = threadIdx.x; o < BB; o += blockDim.x) {
+      Sd[o] = Ad[o];
+      Inv[o] = (o % B) == (o / B) ? 1. : 0.;
+    }
+    __syncthreads();
+    const bool ok = cta_lu_solve<RMAX>(Sd, B, Inv, B, B, B, piv_s, inv_piv, bcast);
+    if (!ok && threadIdx.x == 0) raise_err(a.err, DERR_SINGULAR_ILU);
+    double *Di = a.dinv + (size_t)i * BB;
+    for (int o = threadIdx.x; o < BB; o += blockDim.x) Di[o] = Inv[o];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(a.progress + g, a.tag | (unsigned long long)(slot + 1));
+  }
+}
+
+// ------------------------------------------------------------ fill kernels
+// HDG: all 16 panels C_s R_s X_{:,o} of every cell (FaceCoupling::Panel,
+// src/operators.cpp:7-26), layout [cell][s][o][t x t column-major].
+template <int Q>
+__global__ void __launch_bounds__(256)
+    ilu_panels_kernel(Geo g, const double *__restrict__ tab, const double *__restrict__ XY,
+                      const double *__restrict__ Cb, double *__restrict__ panels16) {
+  constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, TT = T * T;
+  __shared__ STab<Q> st;
+  load_tables<Q>(st, tab);
+  __syncthreads();
+  const long long total = (long long)g.n * 16 * TT;
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(o / (16 * TT)), rem = (int)(o % (16 * TT));
+    const int pan = rem / TT, r2 = rem % TT;
+    const int row = r2 % T, cc = r2 / T;
+    const int s = pan >> 2, so = pan & 3, jj = row >> 2, c = row & 3;
+    const double *xc = XY + (size_t)e * M * NR + (size_t)(so * T + cc) * M;
+    double val[4] = {0., 0., 0., 0.};
+    for (int l = 0; l < Q; ++l) {
+      const double f = st.fb(s, jj, l);
+      const double *xv = xc + 4 * line_node<Q>(s, jj, l);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) val[d] += f * xv[d];
+    }
+    const double *cb = Cb + ((size_t)e * 4 * Q + s * Q + jj) * 16;
+    double res = 0.;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
+    panels16[o] = res;
+  }
+}
+
+// HDG block (f, g) = delta_fg D_f - sum over cells holding both faces of the
+// cell's panel (side of f, side of g), in cell order (operators.cpp:48-74).
+__global__ void __launch_bounds__(256)
+    ilu_fill_hdg_kernel(int nnzb, int T, const int *__restrict__ erow, const int *__restrict__ col,
+                        const int *__restrict__ fill_ptr, const int *__restrict__ fill_src,
+                        const double *__restrict__ D, const double *__restrict__ panels16,
+                        double *__restrict__ data) {
+  const int TT = T * T;
+  const long long total = (long long)nnzb * TT;
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(o / TT), r2 = (int)(o % TT);
+    const int row = r2 % T, cc = r2 / T;
+    const int f = erow[b];
+    double v = (f == col[b] && row == cc) ? D[(size_t)f * T + row] : 0.;
+    for (int p = fill_ptr[b]; p < fill_ptr[b + 1]; ++p) v = v - panels16[(size_t)fill_src[p] * TT + r2];
+    data[o] = v;
+  }
+}
+
+// DG blocks (PartialDGOperator::FillBlocks, src/partial.cpp:140-170): the
+// diagonal is the cell block of block Jacobi; an off-diagonal block (a, b)
+// holds, for every face joining a and b (in face order), +scale M^-1 phi phi jr
+// when a is the face's left cell and -scale M^-1 phi phi jl when it is the
+// right one. One CTA per block.
+template <int Q>
+__global__ void __launch_bounds__(256)
+    ilu_fill_dg_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                       int nnzb, const int *__restrict__ erow, const int *__restrict__ col,
+                       const int *__restrict__ fill_ptr, const int *__restrict__ fill_src, double *data) {
+  constexpr int P = Q * Q, M = 4 * P;
+  __shared__ STab<Q> st;
+  __shared__ double us[M], UT[16 * Q], FM[4 * Q * 16];
+  load_tables<Q>(st, tab);
+  for (int b = blockIdx.x; b < nnzb; b += gridDim.x) {
+    __syncthreads();
+    const int ea = erow[b], eb = col[b];
+    double *A = data + (size_t)b * M * M;
+    if (ea == eb) {
+      for (int i = threadIdx.x; i < M; i += blockDim.x) us[i] = u[(size_t)ea * M + i];
+      __syncthreads();
+      cell_traces<Q>(st, us, UT);
+      __syncthreads();
+      dg_face_matrices<Q>(UT, FM, g, fz, ea);
+      __syncthreads();
+      build_cell_matrix<Q>(A, M, st, us, FM, g);
+      continue;
+    }
+    for (int o = threadIdx.x; o < M * M; o += blockDim.x) A[o] = 0.;
+    __syncthreads();
+    for (int p = fill_ptr[b]; p < fill_ptr[b + 1]; ++p) {
+      const int code = fill_src[p];
+      const int f = code >> 1;
+      const bool right = (code & 1) != 0;  // block row cell is the face's right cell
+      const int L = f >> 1, axis = f & 1, ls = axis ? 3 : 1, rs = ls - 1;
+      const int R = neighbour(L, ls, g.nx, g.ny);
+      const int ts = right ? rs : ls, trs = right ? ls : rs, tc = right ? L : R;
+      const double len = axis ? g.hx : g.hy;
+      for (int j = threadIdx.x; j < Q; j += blockDim.x) {
+        double tr[4], jm[16];
+        trace4<Q>(st, u, tc, trs, j, tr);
+        jacobian(tr, axis, g.gm1, jm);
+        const int fi = f * Q + j;
+        const double wgt = right ? fz.lw[fi] : fz.rw[fi], pen = right ? fz.pen[fi] : -fz.pen[fi];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) FM[j * 16 + k] = wgt * jm[k] + ((k % 5) == 0 ? pen : 0.);
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < Q * Q * Q * 16; t += blockDim.x) {
+        const int j = t / (Q * Q * 16), rem = t % (Q * Q * 16);
+        const int li = rem / (Q * 16), lk = (rem / 16) % Q, cd = rem % 16, c = cd & 3, d = cd >> 2;
+        const int i = line_node<Q>(ts, j, li), kk = line_node<Q>(trs, j, lk);
+        const double scale = g.dt * len / g.area * st.ew(j);
+        const double w = (right ? -scale : scale) * st.inv_mass(i) * st.fb(ts, j, li) * st.fb(trs, j, lk);
+        A[(size_t)(4 * kk + d) * M + 4 * i + c] += w * FM[j * 16 + c + 4 * d];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+int sm_count_ilu() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// ------------------------------------------------------------ host: plan
+void build_plan(Ctx &c, int form) {
+  IluPlan &P = c.ilu[form];
+  if (P.built) return;
+  const bool hdg = form == EG_FORM_HDG;
+  const int nx = c.desc.nx, ny = c.desc.ny;
+  P.rows = hdg ? c.nf : c.n;
+  P.B = hdg ? c.t : c.m;
+  P.chunk = hdg ? 2 * nx : nx;
+  P.chunks = ny;
+  // Problem::SolverGraph (src/block_ilu.cpp:110-124) plus the row itself
+  std::vector<std::vector<int>> graph(P.rows);
+  if (hdg) {
+    for (int e = 0; e < c.n; ++e)
+      for (int s = 0; s < 4; ++s)
+        for (int o = 0; o < 4; ++o) graph[cell_face(e, s, nx, ny)].push_back(cell_face(e, o, nx, ny));
+  } else {
+    for (int e = 0; e < c.n; ++e) graph[e].push_back(e);
+    for (int f = 0; f < c.nf; ++f) {
+      const int L = f >> 1, R = neighbour(L, (f & 1) ? 3 : 1, nx, ny);
+      graph[L].push_back(R);
+      graph[R].push_back(L);
+    }
+  }
+  std::vector<int> row(1, 0), col, diag(P.rows), erow;
+  for (int i = 0; i < P.rows; ++i) {
+    auto &r = graph[i];
+    r.push_back(i);
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    for (int j : r) {
+      if (j == i) diag[i] = (int)col.size();
+      col.push_back(j);
+      erow.push_back(i);
+    }
+    row.push_back((int)col.size());
+  }
+  P.nnzb = (int)col.size();
+  // retained ILU(0) products (src/block_ilu.cpp:46-57)
+  std::vector<int> upd_ptr(1, 0), upd;
+  for (int i = 0; i < P.rows; ++i) {
+    for (int ik = row[i]; ik < row[i + 1]; ++ik) {
+      if (ik < diag[i]) {
+        const int k = col[ik];
+        int ij = ik + 1, kj = diag[k] + 1;
+        while (ij < row[i + 1] && kj < row[k + 1]) {
+          if (col[ij] < col[kj]) {
+            ++ij;
+          } else if (col[kj] < col[ij]) {
+            ++kj;
+          } else {
+            upd.push_back(ij);
+            upd.push_back(kj);
+            ++ij;
+            ++kj;
+          }
+        }
+      }
+      upd_ptr.push_back((int)upd.size() / 2);
+    }
+  }
+  auto at = [&](int i, int j) {
+    const auto it = std::lower_bound(col.begin() + row[i], col.begin() + row[i + 1], j);
+    return (int)(it - col.begin());
+  };
+  // fill contributions per entry
+  std::vector<std::vector<int>> contrib(P.nnzb);
+  if (hdg) {
+    for (int e = 0; e < c.n; ++e)
+      for (int s = 0; s < 4; ++s)
+        for (int o = 0; o < 4; ++o)
+          contrib[at(cell_face(e, s, nx, ny), cell_face(e, o, nx, ny))].push_back(e * 16 + s * 4 + o);
+  } else {
+    for (int f = 0; f < c.nf; ++f) {
+      const int L = f >> 1, R = neighbour(L, (f & 1) ? 3 : 1, nx, ny);
+      contrib[at(L, R)].push_back(2 * f);
+      contrib[at(R, L)].push_back(2 * f + 1);
+    }
+  }
+  std::vector<int> fill_ptr(1, 0), fill_src;
+  for (auto &v : contrib) {
+    fill_src.insert(fill_src.end(), v.begin(), v.end());
+    fill_ptr.push_back((int)fill_src.size());
+  }
+  if (fill_src.empty()) fill_src.push_back(0);
+  if (upd.empty()) upd.push_back(0);
+  P.maxl = P.maxu = 0;
+  for (int i = 0; i < P.rows; ++i) {
+    P.maxl = std::max(P.maxl, diag[i] - row[i]);
+    P.maxu = std::max(P.maxu, row[i + 1] - diag[i] - 1);
+  }
+  auto upload = [&](const std::vector<int> &v) {
+    int *d = c.alloc_n<int>(v.size());
+    EG_CUDA(cudaMemcpy(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice));
+    return d;
+  };
+  P.row = upload(row);
+  P.col = upload(col);
+  P.diag = upload(diag);
+  P.erow = upload(erow);
+  P.upd_ptr = upload(upd_ptr);
+  P.upd = upload(upd);
+  P.fill_ptr = upload(fill_ptr);
+  P.fill_src = upload(fill_src);
+  const size_t BB = (size_t)P.B * P.B;
+  P.data = c.alloc_n<double>((size_t)P.nnzb * BB);
+  P.dinv = c.alloc_n<double>((size_t)P.rows * BB);
+  P.w = c.alloc_n<double>((size_t)P.rows * P.B);
+  if (hdg) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
+  // launch shapes (cooperative: every CTA of a sweep is resident)
+  const int sms = sm_count_ilu();
+  const int S = (P.B + 31) / 32;
+  const bool staged = P.B <= kStageMaxB;
+  int W = 8;
+  auto sweep_smem = [&](int w) {
+    return sizeof(double) * ((size_t)w * (staged ? kStageBlocks * BB : 0) + (size_t)w * 32 * S);
+  };
+  while (W > 1 && sweep_smem(W) > kSweepSmemBudget) --W;
+  P.sweep_warps = W;
+  P.sweep_smem = sweep_smem(W);
+  P.stage_doubles = staged ? 1 : 0;
+  P.grid_sweep = std::min(P.chunks, sms);  // refined against occupancy at launch
+  P.grid_factor = std::min(P.chunks, sms);
+  P.progress = c.alloc_n<unsigned long long>(std::max(P.grid_sweep, P.grid_factor) + 1);
+  EG_CUDA(cudaMemset(P.progress, 0, sizeof(unsigned long long) * (std::max(P.grid_sweep, P.grid_factor) + 1)));
+  P.abort = c.alloc_n<int>(1);
+  EG_CUDA(cudaMemset(P.abort, 0, sizeof(int)));
+  if (P.B > kStageMaxB) P.work = c.alloc_n<double>((size_t)P.grid_factor * 3 * BB);
+  P.epoch = 0;
+  P.built = true;
+}
+
+template <class Kern, class Args>
+void launch_coop(Kern kern, int grid, int block, size_t smem, cudaStream_t s, Args &args) {
+  void *params[] = {&args};
+  EG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), grid, block, params, smem, s));
+}
+
+// Largest grid not above `want` whose CTAs are all resident at once.
+template <class Kern>
+int coop_grid(Kern kern, int block, size_t smem, int want) {
+  if (smem > 48 * 1024)
+    EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  EG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem));
+  if (per_sm < 1) fail(EG_ERR_INVALID, "block ILU sweep does not fit on an SM");
+  return std::min(want, per_sm * sm_count_ilu());
+}
+
+template <int S, bool BACK>
+void sweep(Ctx &c, IluPlan &P, const double *in, double *out) {
+  auto kern = ilu_sweep_kernel<S, BACK>;
+  const int block = 32 * P.sweep_warps;
+  const int grid = coop_grid(kern, block, P.sweep_smem, P.grid_sweep);
+  SweepArgs a{};
+  a.sc = Sched{P.chunk, P.chunks, grid};
+  a.B = P.B;
+  a.row = P.row;
+  a.col = P.col;
+  a.diag = P.diag;
+  a.data = P.data;
+  a.dinv = P.dinv;
+  a.in = in;
+  a.out = out;
+  a.progress = P.progress;
+  a.abort = P.abort;
+  a.err = c.derr;
+  a.tag = (unsigned long long)(++P.epoch) << 32;
+  a.staged = P.stage_doubles;
+  launch_coop(kern, grid, block, P.sweep_smem, c.stream, a);
+}
+
+template <bool BACK>
+void sweep_dispatch(Ctx &c, IluPlan &P, const double *in, double *out) {
+  switch ((P.B + 31) / 32) {
+    case 1: sweep<1, BACK>(c, P, in, out); break;
+    case 2: sweep<2, BACK>(c, P, in, out); break;
+    case 3: sweep<3, BACK>(c, P, in, out); break;
+    case 4: sweep<4, BACK>(c, P, in, out); break;
+    case 5: sweep<5, BACK>(c, P, in, out); break;
+    case 6: sweep<6, BACK>(c, P, in, out); break;
+    case 7: sweep<7, BACK>(c, P, in, out); break;
+    case 8: sweep<8, BACK>(c, P, in, out); break;
+    case 9: sweep<9, BACK>(c, P, in, out); break;
+    case 10: sweep<10, BACK>(c, P, in, out); break;
+    case 11: sweep<11, BACK>(c, P, in, out); break;
+    default: fail(EG_ERR_INVALID, "unsupported block size");
+  }
+}
+
+template <int RMAX, bool SMEM>
+void factor_launch(Ctx &c, IluPlan &P) {
+  auto kern = ilu_factor_kernel<RMAX, SMEM>;
+  const size_t smem = SMEM ? sizeof(double) * 3 * (size_t)P.B * P.B : 0;
+  const int grid = coop_grid(kern, 256, smem, P.grid_factor);
+  FactorArgs a{};
+  a.sc = Sched{P.chunk, P.chunks, grid};
+  a.B = P.B;
+  a.row = P.row;
+  a.col = P.col;
+  a.diag = P.diag;
+  a.upd_ptr = P.upd_ptr;
+  a.upd = P.upd;
+  a.data = P.data;
+  a.dinv = P.dinv;
+  a.work = P.work;
+  a.progress = P.progress;
+  a.abort = P.abort;
+  a.err = c.derr;
+  a.tag = (unsigned long long)(++P.epoch) << 32;
+  launch_coop(kern, grid, 256, smem, c.stream, a);
+}
+
+void factor_dispatch(Ctx &c, IluPlan &P) {
+  if (P.B <= kStageMaxB) {
+    if (P.B <= 32) factor_launch<1, true>(c, P);
+    else factor_launch<2, true>(c, P);
+    return;
+  }
+  switch ((P.B + 31) / 32) {
+    case 2: factor_launch<2, false>(c, P); break;
+    case 3: factor_launch<3, false>(c, P); break;
+    case 4: factor_launch<4, false>(c, P); break;
+    case 5: factor_launch<5, false>(c, P); break;
+    case 6: factor_launch<6, false>(c, P); break;
+    case 7: factor_launch<7, false>(c, P); break;
+    case 8: factor_launch<8, false>(c, P); break;
+    case 9: factor_launch<9, false>(c, P); break;
+    case 10: factor_launch<10, false>(c, P); break;
+    case 11: factor_launch<11, false>(c, P); break;
+    default: fail(EG_ERR_INVALID, "unsupported block size");
+  }
+}
+
+}  // namespace
+
+void ilu_refresh(Ctx &c, int form, bool factor) {
+  build_plan(c, form);
+  IluPlan &P = c.ilu[form];
+  const bool hdg = form == EG_FORM_HDG;
+  if (hdg && !c.condensed) fail(EG_ERR_INVALID, "Schur preconditioner requires a condensation");
+  ProfScope ps(c, hdg ? EG_K_SCHUR_JACOBI : EG_K_DG_JACOBI, factor ? 3 : 2);
+  EG_CUDA(cudaMemsetAsync(P.abort, 0, sizeof(int), c.stream));
+  const int sms = sm_count_ilu();
+  if (hdg) {
+    const long long np = (long long)c.n * 16 * c.t * c.t;
+    const int grid = (int)std::min<long long>((np + 255) / 256, (long long)sms * 16);
+    EG_DISPATCH_Q(c.q, (ilu_panels_kernel<Q><<<grid, 256, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb, P.panels16)));
+    EG_CUDA(cudaGetLastError());
+    const long long ne = (long long)P.nnzb * c.t * c.t;
+    const int g2 = (int)std::min<long long>((ne + 255) / 256, (long long)sms * 16);
+    ilu_fill_hdg_kernel<<<g2, 256, 0, c.stream>>>(P.nnzb, c.t, P.erow, P.col, P.fill_ptr, P.fill_src, c.D,
+                                                  P.panels16, P.data);
+  } else {
+    const int grid = std::min(P.nnzb, sms * 8);
+    EG_DISPATCH_Q(c.q, (ilu_fill_dg_kernel<Q><<<grid, 256, 0, c.stream>>>(
+                           c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, c.u, P.nnzb, P.erow, P.col,
+                           P.fill_ptr, P.fill_src, P.data)));
+  }
+  EG_CUDA(cudaGetLastError());
+  if (factor) factor_dispatch(c, P);
+}
+
+void launch_ilu_apply(Ctx &c, int form, const double *b, double *x) {
+  IluPlan &P = c.ilu[form];
+  if (!P.built) fail(EG_ERR_INVALID, "no preconditioner built");
+  ProfScope ps(c, EG_K_PC_APPLY, 2);
+  sweep_dispatch<false>(c, P, b, P.w);
+  sweep_dispatch<true>(c, P, P.w, x);
+}
+
+}  // namespace eg

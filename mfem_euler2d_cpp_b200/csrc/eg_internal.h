@@ -97,6 +97,25 @@ struct LinearOps {
   virtual ~LinearOps() = default;
 };
 
+// Block ILU(0) of one form (FixedBlockILU, src/block_ilu.cpp:10-109): fixed
+// BSR structure in natural order, numeric blocks and the explicit inverses of
+// the factored diagonal blocks. Built on first use (eg_ilu.cu).
+struct IluPlan {
+  bool built = false;
+  int rows = 0, B = 0, nnzb = 0, chunk = 0, chunks = 0, maxl = 0, maxu = 0;
+  int *row = nullptr, *col = nullptr, *diag = nullptr, *erow = nullptr;
+  int *upd_ptr = nullptr, *upd = nullptr;        // per entry: (target, upper) pairs
+  int *fill_ptr = nullptr, *fill_src = nullptr;  // per entry: fill contributions
+  double *data = nullptr, *dinv = nullptr, *w = nullptr;
+  double *panels16 = nullptr;                    // HDG: 16 panels C_s X_o per cell
+  double *work = nullptr;                        // factor slab for large blocks
+  unsigned long long *progress = nullptr;        // one counter per CTA of a sweep
+  int *abort = nullptr;
+  unsigned epoch = 0;
+  int grid_factor = 0, grid_sweep = 0, sweep_warps = 0, stage_doubles = 0;
+  size_t sweep_smem = 0;
+};
+
 struct Ctx {
   eg_desc desc{};
   eg_opts opts{};
@@ -147,6 +166,8 @@ struct Ctx {
   double last_residual_s = 0.;
   bool update_timer_open = false;
 
+  IluPlan ilu[2];  // per form (EG_FORM_DG, EG_FORM_HDG)
+
   bool residual_ready = false;
   bool condensed = false;
   Profiler prof;
@@ -182,6 +203,11 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er);
 void launch_schur_jacobi(Ctx &c, bool factor);
 // x = Inv b for explicit block inverses (Schur block Jacobi apply).
 void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x);
+// ---- block ILU(0) (eg_ilu.cu) ----
+// Fill (and with factor set, factor) the ILU of `form` at the current state /
+// condensation; x = ILU^{-1} b.
+void ilu_refresh(Ctx &c, int form, bool factor);
+void launch_ilu_apply(Ctx &c, int form, const double *b, double *x);
 // ---- launchers (eg_krylov.cu) ----
 // Weighted squared norm sum(metric * x * x) into dscal[slot] (device).
 void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot);
