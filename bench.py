@@ -252,6 +252,7 @@ def timed_updates(ctx, stepper, K, world, events_stream, host_io=None):
 
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     device_ms = 0.0
+    krylov = 0
     barrier(world)
     torch.cuda.synchronize()
     start.record(events_stream)
@@ -262,12 +263,14 @@ def timed_updates(ctx, stepper, K, world, events_stream, host_io=None):
         if st is None:
             raise RuntimeError("schedule exhausted")
         device_ms += st.device_ms
+        krylov += st.krylov_iterations
         if host_io is not None:
             ctx.download_ptr("U", host_io[1].ctypes.data)
     end.record(events_stream)
     end.synchronize()
     torch.cuda.synchronize()
     barrier(world)
+    timed_updates.krylov = krylov
     return start.elapsed_time(end), device_ms
 
 
@@ -329,6 +332,7 @@ def run_ours(args, world, rank, local):
     sampler.start()
     time.sleep(0.3)
     elapsed_ms, dev_ms = timed_updates(ctx, stepper, K, world, ext)
+    krylov_main = timed_updates.krylov
     clocks = sampler.stop()
     launches = ctx.lib.eg_launch_count(ctx.h) - launches0
     prof = {}
@@ -365,9 +369,38 @@ def run_ours(args, world, rank, local):
         dg_ms, dg_dev = timed_updates(ctxd, std, K, world, extd)
         dg_ms = max_over_ranks(world, dg_ms)
         dg = {"value": dg_ms * 1e-3 / (K * world), "unit": "s", "ms_per_step": dg_ms / K,
-              "mean_newton_device_s": dg_dev * 1e-3 / K, "form": "dg"}
+              "mean_newton_device_s": dg_dev * 1e-3 / K, "form": "dg",
+              "krylov_per_update": timed_updates.krylov / K}
         std.close()
         ctxd.close()
+
+    # the same HDG workload preconditioned by block ILU(0) (secondary line)
+    ilu = None
+    if not args.no_ilu:
+        wi = dict(w, precond="block-ilu0")
+        ctxi = make_context(wi, "hdg", local)
+        sti = make_stepper(ctxi, wi, W + K, "hdg")
+        exti = torch.cuda.ExternalStream(ctxi.stream_ptr())
+        for _ in range(W):
+            sti.next()
+        ctxi.lib.eg_profile_reset(ctxi.h)
+        ctxi.lib.eg_profile_enable(ctxi.h, 1)
+        il_ms, il_dev = timed_updates(ctxi, sti, K, world, exti)
+        il_kry = timed_updates.krylov
+        il_prof = {}
+        for i, name in enumerate(K_NAMES):
+            import ctypes as C
+
+            ms, cnt = C.c_double(), C.c_longlong()
+            ctxi.lib.eg_profile_query(ctxi.h, i, C.byref(ms), C.byref(cnt))
+            if cnt.value:
+                il_prof[name] = round(ms.value / K, 3)
+        il_ms = max_over_ranks(world, il_ms)
+        ilu = {"value": il_ms * 1e-3 / (K * world), "unit": "s", "ms_per_step": il_ms / K,
+               "mean_newton_device_s": il_dev * 1e-3 / K, "precond": "block-ilu0",
+               "krylov_per_update": il_kry / K, "kernel_ms_per_update": il_prof}
+        sti.close()
+        ctxi.close()
 
     if rank != 0:
         return None
@@ -420,6 +453,11 @@ def run_ours(args, world, rank, local):
                    "per_update_s": times}
         else:
             cpu = {"value": None, "unit": "s", "cores": 1, "kind": "reference", "sample": f"unavailable: {src}"}
+        if ilu is not None:
+            times_i, _ = run_reference_updates(dict(w, precond="block-ilu0"), 1)
+            if times_i:
+                ilu["cpu_reference_s"] = float(np.mean(times_i))
+                ilu["cpu_reference_per_update_s"] = times_i
     value = elapsed_ms * 1e-3 / (K * world)
     line = {
         "metric": f"{METRIC} (HDG, {w['nx']}x{w['ny']} Q{w['k']}, block-Jacobi)",
@@ -443,10 +481,12 @@ def run_ours(args, world, rank, local):
         "hbm_kernels": hbm_lines,
         "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]},
         "kernel_launches": {k: v[1] for k, v in prof.items() if v[1]},
+        "krylov_per_update": krylov_main / K,
         "gpu_launches": int(launches),
         "cpu_baseline": cpu,
         "clocks": clocks,
         "dg": dg,
+        "ilu": ilu,
     }
     return line
 
@@ -491,6 +531,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--no-dg", action="store_true", help="skip the secondary DG-form measurement")
+    ap.add_argument("--no-ilu", action="store_true", help="skip the secondary block-ILU(0) measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-updates", type=int, default=12)
     args = ap.parse_args()

@@ -19,6 +19,7 @@ from . import capi
 
 OPS = ("condense", "schur_apply", "recover", "pc_factor", "pc_apply", "dg_apply", "residual",
        "linear_solve", "dg_jacobi")
+PRECONDS = {"block-jacobi": capi.PC_JACOBI, "block-ilu0": capi.PC_ILU0}
 
 
 def main(argv=None):
@@ -29,11 +30,17 @@ def main(argv=None):
     ap.add_argument("--alpha", type=float, default=30.0)
     ap.add_argument("--op", choices=OPS, default="condense")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--precond", choices=sorted(PRECONDS), default="block-jacobi")
+    ap.add_argument("--form", choices=("dg", "hdg"), default=None,
+                    help="form of the context (default: dg for dg_apply/dg_jacobi, hdg otherwise)")
     args = ap.parse_args(argv)
     lib = capi.load()
-    form = capi.FORM_DG if args.op in ("dg_apply", "dg_jacobi") else capi.FORM_HDG
+    if args.form is None:
+        form = capi.FORM_DG if args.op in ("dg_apply", "dg_jacobi") else capi.FORM_HDG
+    else:
+        form = capi.FORM_DG if args.form == "dg" else capi.FORM_HDG
     d = capi.simple_wave_desc(args.nx, args.ny, args.k, args.alpha)
-    with capi.Context(d, capi.default_opts(form=form)) as ctx:
+    with capi.Context(d, capi.default_opts(form=form, precond=PRECONDS[args.precond])) as ctx:
         ctx.initial()
         rate = ctx.freeze(1e-3)
         dt = 0.24169426078821 / rate  # first SSP-DIRK3 stage at CFL 1
@@ -72,7 +79,8 @@ def main(argv=None):
         names = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "recover",
                  "recovered_residual", "schur_jacobi", "pc_apply", "krylov", "freeze", "admissible",
                  "vector"]
-        out = {"op": args.op, "nx": args.nx, "ny": args.ny, "k": args.k, "reps": args.reps}
+        out = {"op": args.op, "nx": args.nx, "ny": args.ny, "k": args.k, "reps": args.reps,
+               "precond": args.precond}
         for i, name in enumerate(names):
             ms, cnt = C.c_double(), C.c_longlong()
             lib.eg_profile_query(ctx.h, i, C.byref(ms), C.byref(cnt))
