@@ -39,16 +39,14 @@ constexpr unsigned kSpinLimit = 1u << 24;  // polls per wait, each with a short 
 constexpr unsigned kCopySpinLimit = 1u << 16;  // try_wait itself suspends between polls
 constexpr int kStageBlocks = 4;             // blocks staged per warp and row
 constexpr int kStageMaxB = 36;              // larger blocks are read from global memory
-constexpr size_t kSweepSmemBudget = 200 * 1024;
+constexpr size_t kSweepSmemBudget = 210 * 1024;
+constexpr size_t kRingBytes = 48 * 1024;    // shared-memory ring of finished rows per CTA
 
 // ------------------------------------------------------------ sync helpers
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
-}
-__device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 
@@ -112,33 +110,25 @@ __device__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
 }
 
 // ------------------------------------------------------------- scheduling
-struct Sched {
-  int chunk, chunks, G;
-};
-__device__ __forceinline__ int owned_chunks(const Sched &s, int g) { return (s.chunks - g + s.G - 1) / s.G; }
-template <bool BACK>
-__device__ __forceinline__ int slot_row(const Sched &s, int g, int K, int slot) {
-  const int k = slot / s.chunk, o = slot % s.chunk;
-  if (!BACK) return (g + k * s.G) * s.chunk + o;
-  return (g + (K - 1 - k) * s.G) * s.chunk + (s.chunk - 1 - o);
-}
-template <bool BACK>
-__device__ __forceinline__ void row_owner(const Sched &s, int j, int &owner, int &slot) {
-  const int c = j / s.chunk, o = j % s.chunk, k = c / s.G;
-  owner = c % s.G;
-  if (!BACK) {
-    slot = k * s.chunk + o;
-  } else {
-    const int K = owned_chunks(s, owner);
-    slot = (K - 1 - k) * s.chunk + (s.chunk - 1 - o);
-  }
+// Rows of one sweep, host-built for a fixed grid G: chunk c (one grid row of
+// faces or cells) belongs to CTA c mod G, whose slots walk its rows in
+// increasing (forward, factor) or decreasing (backward) order. For every
+// slot the table holds (row, first entry, entry count) and, for each entry
+// the sweep reads, its producer (owner CTA << 22 | owner slot) and row.
+constexpr int kMaxDeps = 8;
+constexpr int kOwnerShift = 22;
+constexpr int kSlotMask = (1 << kOwnerShift) - 1;
+
+__device__ __forceinline__ void publish_max(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.max.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // ------------------------------------------------------------ sweep kernel
 struct SweepArgs {
-  Sched sc;
-  int B;
-  const int *row, *col, *diag;
+  int B, ring;
+  const int *slot_ptr;
+  const int4 *meta;
+  const int2 *deps;
   const double *data, *dinv;
   const double *in;  // forward: b; backward: the forward result w
   double *out;       // forward: w; backward: x
@@ -150,31 +140,46 @@ struct SweepArgs {
 
 // FixedBlockILU::Mult (src/block_ilu.cpp:88-109). Forward: w_i = b_i -
 // sum_{j<i} L_ij w_j. Backward: x_i = U_ii^{-1} (w_i - sum_{j>i} U_ij x_j).
-// One warp per row, lanes own block rows r = lane + 32 s; W warps per CTA keep
-// W rows (and their block copies) in flight; rows are published in order.
+// One warp per row (lanes own block rows r = lane + 32 s); the W warps of a
+// CTA keep W rows and their block copies in flight. A finished row goes to a
+// shared-memory ring (read by later rows of the same CTA) and to global
+// memory; the CTA's own count is published first, then, off the local chain,
+// the release of the global counter that other CTAs poll.
 template <int S, bool BACK>
-__global__ void __launch_bounds__(256) ilu_sweep_kernel(SweepArgs a) {
+__global__ void __launch_bounds__(256, 1) ilu_sweep_kernel(SweepArgs a) {
   extern __shared__ __align__(128) double smem[];
   __shared__ unsigned done_local;
   __shared__ __align__(8) unsigned long long bars[8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
   const int g = blockIdx.x, B = a.B;
   const size_t BB = (size_t)B * B;
-  const int K = owned_chunks(a.sc, g), nslots = K * a.sc.chunk;
+  const int p0 = a.slot_ptr[g], nslots = a.slot_ptr[g + 1] - p0;
   const size_t stage_doubles = a.staged ? kStageBlocks * BB : 0;
   double *stage = smem + (size_t)warp * stage_doubles;
   double *vb = smem + (size_t)W * stage_doubles + (size_t)warp * 32 * S;
+  double *ring = smem + (size_t)W * (stage_doubles + 32 * S);
   if (threadIdx.x == 0) done_local = 0;
   if (a.staged && lane == 0) mbar_init(&bars[warp]);
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
   volatile unsigned *dl = &done_local;
   unsigned phase = 0;
+  int4 nm = make_int4(0, 0, 0, 0);
+  int2 nd[kMaxDeps];
+  auto fetch = [&](int slot) {
+    if (slot < nslots) {
+      nm = a.meta[p0 + slot];
+#pragma unroll
+      for (int k = 0; k < kMaxDeps; ++k) nd[k] = a.deps[(size_t)(p0 + slot) * kMaxDeps + k];
+    }
+  };
+  fetch(warp);
   for (int slot = warp; slot < nslots; slot += W) {
-    const int i = slot_row<BACK>(a.sc, g, K, slot);
-    const int e0 = BACK ? a.diag[i] + 1 : a.row[i];
-    const int e1 = BACK ? a.row[i + 1] : a.diag[i];
-    const int ne = e1 - e0;
+    const int i = nm.x, e0 = nm.y, ne = nm.z;
+    int2 dep[kMaxDeps];
+#pragma unroll
+    for (int k = 0; k < kMaxDeps; ++k) dep[k] = nd[k];
+    fetch(slot + W);  // the next row's schedule is in flight during this row
     const int nst = a.staged ? min(ne, BACK ? kStageBlocks - 1 : kStageBlocks) : 0;
     const bool copy = a.staged && (nst > 0 || BACK);
     if (copy && lane == 0) {
@@ -200,27 +205,32 @@ __global__ void __launch_bounds__(256) ilu_sweep_kernel(SweepArgs a) {
       phase ^= 1u;
     }
     bool ok = true;
-    for (int e = e0; e < e1; ++e) {
-      const int j = a.col[e];
-      int owner, js;
-      row_owner<BACK>(a.sc, j, owner, js);
-      ok = owner == g ? wait_local(dl, (unsigned)js + 1, a.abort, a.err)
-                      : wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
-      if (!ok) break;
-      __threadfence_block();
-      for (int r = lane; r < B; r += 32) vb[r] = __ldcg(a.out + (size_t)j * B + r);
-      __syncwarp();
-      const double *A = e - e0 < nst ? stage + (size_t)(e - e0) * BB : a.data + (size_t)e * BB;
 #pragma unroll
-      for (int s = 0; s < S; ++s) {
-        const int r = lane + 32 * s;
-        if (r < B) {
-          double t = acc[s];
-          for (int cc = 0; cc < B; ++cc) t -= A[(size_t)cc * B + r] * vb[cc];
-          acc[s] = t;
+    for (int k = 0; k < kMaxDeps; ++k) {
+      if (k < ne && ok) {
+        const int owner = dep[k].x >> kOwnerShift, js = dep[k].x & kSlotMask, j = dep[k].y;
+        const bool local = owner == g;
+        ok = local ? wait_local(dl, (unsigned)js + 1, a.abort, a.err)
+                   : wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
+        if (ok) {
+          __threadfence_block();
+          const bool in_ring = local && slot - js <= a.ring - W;
+          const double *src = ring + (size_t)(js & (a.ring - 1)) * B;
+          for (int r = lane; r < B; r += 32) vb[r] = in_ring ? src[r] : __ldcg(a.out + (size_t)j * B + r);
+          __syncwarp();
+          const double *A = k < nst ? stage + (size_t)k * BB : a.data + (size_t)(e0 + k) * BB;
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            const int r = lane + 32 * s;
+            if (r < B) {
+              double t = acc[s];
+              for (int cc = 0; cc < B; ++cc) t -= A[(size_t)cc * B + r] * vb[cc];
+              acc[s] = t;
+            }
+          }
+          __syncwarp();
         }
       }
-      __syncwarp();
     }
     if (!ok) return;
     if (BACK) {
@@ -242,19 +252,23 @@ __global__ void __launch_bounds__(256) ilu_sweep_kernel(SweepArgs a) {
       }
       __syncwarp();
     }
+    double *rs = ring + (size_t)(slot & (a.ring - 1)) * B;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       const int r = lane + 32 * s;
-      if (r < B) a.out[(size_t)i * B + r] = acc[s];
+      if (r < B) {
+        a.out[(size_t)i * B + r] = acc[s];
+        rs[r] = acc[s];
+      }
     }
-    __threadfence();
+    __threadfence_block();
     __syncwarp();
     int pub = 1;
     if (lane == 0) {
       pub = wait_local(dl, (unsigned)slot, a.abort, a.err);  // rows are published in order
       if (pub) {
         *dl = (unsigned)slot + 1;
-        st_release(a.progress + g, a.tag | (unsigned long long)(slot + 1));
+        publish_max(a.progress + g, a.tag | (unsigned long long)(slot + 1));
       }
     }
     if (!__shfl_sync(0xffffffffu, pub, 0)) return;
@@ -263,9 +277,11 @@ __global__ void __launch_bounds__(256) ilu_sweep_kernel(SweepArgs a) {
 
 // ----------------------------------------------------------- factor kernel
 struct FactorArgs {
-  Sched sc;
-  int B;
-  const int *row, *col, *diag, *upd_ptr, *upd;
+  int B, maxrow, maxupd;
+  const int *slot_ptr;
+  const int4 *meta;   // forward schedule: (row, first lower entry, lower count)
+  const int2 *deps;
+  const int *row, *diag, *upd_ptr, *upd;
   double *data, *dinv, *work;
   unsigned long long *progress;
   int *abort, *err;
@@ -275,9 +291,10 @@ struct FactorArgs {
 // FixedBlockILU::Factor (src/block_ilu.cpp:74-87), one CTA per row: for each
 // lower entry (i,k) in column order, L_ik = A_ik U_kk^{-1}, then A_ij -= L_ik
 // U_kj over the retained products; finally the pivoted LU of the diagonal
-// block, stored as its explicit inverse.
+// block, stored as its explicit inverse. With SMEM the row's blocks, U_kk^{-1}
+// and the U_kj of one step are staged in shared memory.
 template <int RMAX, bool SMEM>
-__global__ void __launch_bounds__(256) ilu_factor_kernel(FactorArgs a) {
+__global__ void __launch_bounds__(256, 1) ilu_factor_kernel(FactorArgs a) {
   extern __shared__ __align__(16) double fsm[];
   __shared__ int piv_s[32 * RMAX];
   __shared__ double inv_piv[32 * RMAX];
@@ -285,47 +302,75 @@ __global__ void __launch_bounds__(256) ilu_factor_kernel(FactorArgs a) {
   __shared__ int stop;
   const int B = a.B;
   const int BB = B * B;
-  const int g = blockIdx.x, K = owned_chunks(a.sc, g), nslots = K * a.sc.chunk;
-  double *Lt = SMEM ? fsm : a.work + (size_t)g * 3 * BB;
-  double *Sd = Lt + BB, *Inv = Sd + BB;
+  const int g = blockIdx.x, p0 = a.slot_ptr[g], nslots = a.slot_ptr[g + 1] - p0;
+  double *Lt, *Sd, *Inv, *rowblk = nullptr, *Dk = nullptr, *Ub = nullptr;
+  if (SMEM) {
+    rowblk = fsm;                         // the row's blocks (maxrow)
+    Dk = rowblk + (size_t)a.maxrow * BB;  // U_kk^{-1}
+    Ub = Dk + BB;                         // the U_kj of one step (maxupd)
+    Lt = Ub + (size_t)a.maxupd * BB;
+  } else {
+    Lt = a.work + (size_t)g * 3 * BB;
+  }
+  Sd = Lt + BB;
+  Inv = Sd + BB;
   for (int slot = 0; slot < nslots; ++slot) {
-    const int i = slot_row<false>(a.sc, g, K, slot);
+    const int4 m = a.meta[p0 + slot];
+    const int i = m.x, rb = a.row[i], re = a.row[i + 1], di = a.diag[i];
     if (threadIdx.x == 0) {
       int ok = 1;
-      for (int e = a.row[i]; e < a.diag[i] && ok; ++e) {
-        int owner, js;
-        row_owner<false>(a.sc, a.col[e], owner, js);
+      for (int k = 0; k < m.z && ok; ++k) {
+        const int2 d = a.deps[(size_t)(p0 + slot) * kMaxDeps + k];
+        const int owner = d.x >> kOwnerShift, js = d.x & kSlotMask;
         if (owner != g) ok = wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
       }
       stop = !ok;
     }
+    if (SMEM)
+      for (int o = threadIdx.x; o < (re - rb) * BB; o += blockDim.x) rowblk[o] = a.data[(size_t)rb * BB + o];
     __syncthreads();
     if (stop) return;
-    for (int ik = a.row[i]; ik < a.diag[i]; ++ik) {
-      const int k = a.col[ik];
-      double *Aik = a.data + (size_t)ik * BB;
-      const double *Dk = a.dinv + (size_t)k * BB;
+    for (int ik = rb; ik < di; ++ik) {
+      const int kk = a.deps[(size_t)(p0 + slot) * kMaxDeps + (ik - rb)].y;
+      const int u0 = a.upd_ptr[ik], nu = a.upd_ptr[ik + 1] - u0;
+      double *Aik = SMEM ? rowblk + (size_t)(ik - rb) * BB : a.data + (size_t)ik * BB;
+      const double *Dsrc = a.dinv + (size_t)kk * BB;
+      if (SMEM) {
+        for (int o = threadIdx.x; o < BB; o += blockDim.x) Dk[o] = __ldcg(Dsrc + o);
+        for (int t = threadIdx.x; t < nu * BB; t += blockDim.x)
+          Ub[t] = __ldcg(a.data + (size_t)a.upd[2 * (u0 + t / BB) + 1] * BB + t % BB);
+        __syncthreads();
+      }
       for (int o = threadIdx.x; o < BB; o += blockDim.x) {
         const int r = o % B, cc = o / B;
         double sum = 0.;
-        for (int s = 0; s < B; ++s) sum += Aik[(size_t)s * B + r] * __ldcg(Dk + (size_t)cc * B + s);
+        if (SMEM) {
+          for (int s = 0; s < B; ++s) sum += Aik[(size_t)s * B + r] * Dk[(size_t)cc * B + s];
+        } else {
+          for (int s = 0; s < B; ++s) sum += Aik[(size_t)s * B + r] * __ldcg(Dsrc + (size_t)cc * B + s);
+        }
         Lt[o] = sum;
       }
       __syncthreads();
       for (int o = threadIdx.x; o < BB; o += blockDim.x) Aik[o] = Lt[o];
-      const int u0 = a.upd_ptr[ik], nu = a.upd_ptr[ik + 1] - u0;
       for (int t = threadIdx.x; t < nu * BB; t += blockDim.x) {
-        const int uu = u0 + t / BB, o = t % BB;
+        const int uu = t / BB, o = t % BB;
         const int r = o % B, cc = o / B;
-        double *T = a.data + (size_t)a.upd[2 * uu] * BB;
-        const double *U = a.data + (size_t)a.upd[2 * uu + 1] * BB;
+        const int target = a.upd[2 * (u0 + uu)];
+        double *T = SMEM ? rowblk + (size_t)(target - rb) * BB : a.data + (size_t)target * BB;
         double sum = 0.;
-        for (int s = 0; s < B; ++s) sum += Lt[(size_t)s * B + r] * __ldcg(U + (size_t)cc * B + s);
+        if (SMEM) {
+          const double *U = Ub + (size_t)uu * BB;
+          for (int s = 0; s < B; ++s) sum += Lt[(size_t)s * B + r] * U[(size_t)cc * B + s];
+        } else {
+          const double *U = a.data + (size_t)a.upd[2 * (u0 + uu) + 1] * BB;
+          for (int s = 0; s < B; ++s) sum += Lt[(size_t)s * B + r] * __ldcg(U + (size_t)cc * B + s);
+        }
         T[o] -= sum;
       }
       __syncthreads();
     }
-    const double *Ad = a.data + (size_t)a.diag[i] * BB;
+    const double *Ad = SMEM ? rowblk + (size_t)(di - rb) * BB : a.data + (size_t)di * BB;
     for (int o = threadIdx.x; o < BB; o += blockDim.x) {
       Sd[o] = Ad[o];
       Inv[o] = (o % B) == (o / B) ? 1. : 0.;
@@ -335,9 +380,11 @@ __global__ void __launch_bounds__(256) ilu_factor_kernel(FactorArgs a) {
     if (!ok && threadIdx.x == 0) raise_err(a.err, DERR_SINGULAR_ILU);
     double *Di = a.dinv + (size_t)i * BB;
     for (int o = threadIdx.x; o < BB; o += blockDim.x) Di[o] = Inv[o];
+    if (SMEM)
+      for (int o = threadIdx.x; o < (re - rb) * BB; o += blockDim.x) a.data[(size_t)rb * BB + o] = rowblk[o];
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) st_release(a.progress + g, a.tag | (unsigned long long)(slot + 1));
+    if (threadIdx.x == 0) publish_max(a.progress + g, a.tag | (unsigned long long)(slot + 1));
   }
 }
 
@@ -468,6 +515,53 @@ int sm_count_ilu() {
 }
 
 // ------------------------------------------------------------ host: plan
+template <class Kern>
+int per_sm(Kern kern, int block, size_t smem) {
+  // the opt-in covers dynamic sizes whose sum with the static shared memory passes 48 KB
+  if (smem > 0) EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int n = 0;
+  EG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, block, smem));
+  return n;
+}
+
+template <int S>
+int sweep_occupancy(int block, size_t smem) {
+  return std::min(per_sm(ilu_sweep_kernel<S, false>, block, smem), per_sm(ilu_sweep_kernel<S, true>, block, smem));
+}
+int sweep_occupancy_dispatch(int S, int block, size_t smem) {
+  switch (S) {
+    case 1: return sweep_occupancy<1>(block, smem);
+    case 2: return sweep_occupancy<2>(block, smem);
+    case 3: return sweep_occupancy<3>(block, smem);
+    case 4: return sweep_occupancy<4>(block, smem);
+    case 5: return sweep_occupancy<5>(block, smem);
+    case 6: return sweep_occupancy<6>(block, smem);
+    case 7: return sweep_occupancy<7>(block, smem);
+    case 8: return sweep_occupancy<8>(block, smem);
+    case 9: return sweep_occupancy<9>(block, smem);
+    case 10: return sweep_occupancy<10>(block, smem);
+    case 11: return sweep_occupancy<11>(block, smem);
+    default: fail(EG_ERR_INVALID, "unsupported block size");
+  }
+}
+int factor_occupancy(int B, bool staged, size_t smem) {
+  if (staged)
+    return B <= 32 ? per_sm(ilu_factor_kernel<1, true>, 256, smem) : per_sm(ilu_factor_kernel<2, true>, 256, smem);
+  switch ((B + 31) / 32) {
+    case 2: return per_sm(ilu_factor_kernel<2, false>, 256, 0);
+    case 3: return per_sm(ilu_factor_kernel<3, false>, 256, 0);
+    case 4: return per_sm(ilu_factor_kernel<4, false>, 256, 0);
+    case 5: return per_sm(ilu_factor_kernel<5, false>, 256, 0);
+    case 6: return per_sm(ilu_factor_kernel<6, false>, 256, 0);
+    case 7: return per_sm(ilu_factor_kernel<7, false>, 256, 0);
+    case 8: return per_sm(ilu_factor_kernel<8, false>, 256, 0);
+    case 9: return per_sm(ilu_factor_kernel<9, false>, 256, 0);
+    case 10: return per_sm(ilu_factor_kernel<10, false>, 256, 0);
+    case 11: return per_sm(ilu_factor_kernel<11, false>, 256, 0);
+    default: fail(EG_ERR_INVALID, "unsupported block size");
+  }
+}
+
 void build_plan(Ctx &c, int form) {
   IluPlan &P = c.ilu[form];
   if (P.built) return;
@@ -507,8 +601,10 @@ void build_plan(Ctx &c, int form) {
   P.nnzb = (int)col.size();
   // retained ILU(0) products (src/block_ilu.cpp:46-57)
   std::vector<int> upd_ptr(1, 0), upd;
+  P.maxupd = 1;
   for (int i = 0; i < P.rows; ++i) {
     for (int ik = row[i]; ik < row[i + 1]; ++ik) {
+      int count = 0;
       if (ik < diag[i]) {
         const int k = col[ik];
         int ij = ik + 1, kj = diag[k] + 1;
@@ -520,11 +616,13 @@ void build_plan(Ctx &c, int form) {
           } else {
             upd.push_back(ij);
             upd.push_back(kj);
+            ++count;
             ++ij;
             ++kj;
           }
         }
       }
+      P.maxupd = std::max(P.maxupd, count);
       upd_ptr.push_back((int)upd.size() / 2);
     }
   }
@@ -553,16 +651,80 @@ void build_plan(Ctx &c, int form) {
   }
   if (fill_src.empty()) fill_src.push_back(0);
   if (upd.empty()) upd.push_back(0);
-  P.maxl = P.maxu = 0;
+  P.maxl = P.maxu = P.maxrow = 0;
   for (int i = 0; i < P.rows; ++i) {
     P.maxl = std::max(P.maxl, diag[i] - row[i]);
     P.maxu = std::max(P.maxu, row[i + 1] - diag[i] - 1);
+    P.maxrow = std::max(P.maxrow, row[i + 1] - row[i]);
   }
+  if (P.maxl > kMaxDeps || P.maxu > kMaxDeps) fail(EG_ERR_INVALID, "block ILU row too long");
+  // launch shapes; every CTA of a sweep must be resident (cooperative launch)
+  const int sms = sm_count_ilu();
+  const size_t BB = (size_t)P.B * P.B;
+  const int S = (P.B + 31) / 32;
+  P.staged = P.B <= kStageMaxB ? 1 : 0;
+  P.ring = 1;
+  while ((size_t)(2 * P.ring) * P.B * sizeof(double) <= kRingBytes) P.ring *= 2;
+  int W = 8;
+  auto sweep_smem = [&](int w) {
+    return sizeof(double) * ((size_t)w * (P.staged ? kStageBlocks * BB : 0) + (size_t)w * 32 * S +
+                             (size_t)P.ring * P.B);
+  };
+  while (W > 1 && sweep_smem(W) > kSweepSmemBudget) --W;
+  if (P.ring < 2 * W) fail(EG_ERR_INVALID, "block ILU ring too small");
+  P.sweep_warps = W;
+  P.sweep_smem = sweep_smem(W);
+  P.factor_smem = P.staged ? sizeof(double) * BB * (size_t)(P.maxrow + P.maxupd + 4) : 0;
+  const int occ = std::min(sweep_occupancy_dispatch(S, 32 * W, P.sweep_smem),
+                           factor_occupancy(P.B, P.staged != 0, P.factor_smem));
+  if (occ < 1) fail(EG_ERR_INVALID, "block ILU kernels do not fit on an SM");
+  const int G = std::min(P.chunks, std::min(occ, 2) * sms);
+  P.grid_sweep = P.grid_factor = G;
+  // schedules (the forward one is also the factor's)
   auto upload = [&](const std::vector<int> &v) {
     int *d = c.alloc_n<int>(v.size());
     EG_CUDA(cudaMemcpy(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice));
     return d;
   };
+  for (int back = 0; back < 2; ++back) {
+    std::vector<int> slot_ptr(G + 1, 0), owner_of(P.rows), slot_of(P.rows);
+    std::vector<std::vector<int>> rows_of(G);
+    for (int g = 0; g < G; ++g) {
+      std::vector<int> chunks;
+      for (int ch = g; ch < P.chunks; ch += G) chunks.push_back(ch);
+      if (back) std::reverse(chunks.begin(), chunks.end());
+      for (int ch : chunks)
+        for (int o = 0; o < P.chunk; ++o) {
+          const int i = ch * P.chunk + (back ? P.chunk - 1 - o : o);
+          owner_of[i] = g;
+          slot_of[i] = (int)rows_of[g].size();
+          rows_of[g].push_back(i);
+        }
+      slot_ptr[g + 1] = slot_ptr[g] + (int)rows_of[g].size();
+    }
+    if (slot_ptr[G] != P.rows) fail(EG_ERR_INVALID, "block ILU schedule does not cover the rows");
+    std::vector<int> meta((size_t)P.rows * 4, 0), deps((size_t)P.rows * kMaxDeps * 2, 0);
+    for (int g = 0; g < G; ++g)
+      for (size_t s = 0; s < rows_of[g].size(); ++s) {
+        const int i = rows_of[g][s];
+        const size_t pos = (size_t)slot_ptr[g] + s;
+        const int e0 = back ? diag[i] + 1 : row[i], e1 = back ? row[i + 1] : diag[i];
+        meta[pos * 4] = i;
+        meta[pos * 4 + 1] = e0;
+        meta[pos * 4 + 2] = e1 - e0;
+        for (int e = e0; e < e1; ++e) {
+          const int j = col[e], k = e - e0;
+          // a row reads only rows that come earlier in its own CTA's order
+          if (owner_of[j] == g && slot_of[j] >= (int)s) fail(EG_ERR_INVALID, "block ILU schedule order");
+          if (slot_of[j] > kSlotMask) fail(EG_ERR_INVALID, "block ILU schedule too long");
+          deps[(pos * kMaxDeps + k) * 2] = (owner_of[j] << kOwnerShift) | slot_of[j];
+          deps[(pos * kMaxDeps + k) * 2 + 1] = j;
+        }
+      }
+    P.slot_ptr[back] = upload(slot_ptr);
+    P.meta[back] = upload(meta);
+    P.deps[back] = upload(deps);
+  }
   P.row = upload(row);
   P.col = upload(col);
   P.diag = upload(diag);
@@ -571,30 +733,15 @@ void build_plan(Ctx &c, int form) {
   P.upd = upload(upd);
   P.fill_ptr = upload(fill_ptr);
   P.fill_src = upload(fill_src);
-  const size_t BB = (size_t)P.B * P.B;
   P.data = c.alloc_n<double>((size_t)P.nnzb * BB);
   P.dinv = c.alloc_n<double>((size_t)P.rows * BB);
   P.w = c.alloc_n<double>((size_t)P.rows * P.B);
   if (hdg) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
-  // launch shapes (cooperative: every CTA of a sweep is resident)
-  const int sms = sm_count_ilu();
-  const int S = (P.B + 31) / 32;
-  const bool staged = P.B <= kStageMaxB;
-  int W = 8;
-  auto sweep_smem = [&](int w) {
-    return sizeof(double) * ((size_t)w * (staged ? kStageBlocks * BB : 0) + (size_t)w * 32 * S);
-  };
-  while (W > 1 && sweep_smem(W) > kSweepSmemBudget) --W;
-  P.sweep_warps = W;
-  P.sweep_smem = sweep_smem(W);
-  P.stage_doubles = staged ? 1 : 0;
-  P.grid_sweep = std::min(P.chunks, sms);  // refined against occupancy at launch
-  P.grid_factor = std::min(P.chunks, sms);
-  P.progress = c.alloc_n<unsigned long long>(std::max(P.grid_sweep, P.grid_factor) + 1);
-  EG_CUDA(cudaMemset(P.progress, 0, sizeof(unsigned long long) * (std::max(P.grid_sweep, P.grid_factor) + 1)));
+  if (!P.staged) P.work = c.alloc_n<double>((size_t)G * 3 * BB);
+  P.progress = c.alloc_n<unsigned long long>(G);
+  EG_CUDA(cudaMemset(P.progress, 0, sizeof(unsigned long long) * G));
   P.abort = c.alloc_n<int>(1);
   EG_CUDA(cudaMemset(P.abort, 0, sizeof(int)));
-  if (P.B > kStageMaxB) P.work = c.alloc_n<double>((size_t)P.grid_factor * 3 * BB);
   P.epoch = 0;
   P.built = true;
 }
@@ -605,28 +752,14 @@ void launch_coop(Kern kern, int grid, int block, size_t smem, cudaStream_t s, Ar
   EG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), grid, block, params, smem, s));
 }
 
-// Largest grid not above `want` whose CTAs are all resident at once.
-template <class Kern>
-int coop_grid(Kern kern, int block, size_t smem, int want) {
-  if (smem > 48 * 1024)
-    EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  EG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem));
-  if (per_sm < 1) fail(EG_ERR_INVALID, "block ILU sweep does not fit on an SM");
-  return std::min(want, per_sm * sm_count_ilu());
-}
-
 template <int S, bool BACK>
 void sweep(Ctx &c, IluPlan &P, const double *in, double *out) {
-  auto kern = ilu_sweep_kernel<S, BACK>;
-  const int block = 32 * P.sweep_warps;
-  const int grid = coop_grid(kern, block, P.sweep_smem, P.grid_sweep);
   SweepArgs a{};
-  a.sc = Sched{P.chunk, P.chunks, grid};
   a.B = P.B;
-  a.row = P.row;
-  a.col = P.col;
-  a.diag = P.diag;
+  a.ring = P.ring;
+  a.slot_ptr = P.slot_ptr[BACK];
+  a.meta = reinterpret_cast<const int4 *>(P.meta[BACK]);
+  a.deps = reinterpret_cast<const int2 *>(P.deps[BACK]);
   a.data = P.data;
   a.dinv = P.dinv;
   a.in = in;
@@ -635,8 +768,8 @@ void sweep(Ctx &c, IluPlan &P, const double *in, double *out) {
   a.abort = P.abort;
   a.err = c.derr;
   a.tag = (unsigned long long)(++P.epoch) << 32;
-  a.staged = P.stage_doubles;
-  launch_coop(kern, grid, block, P.sweep_smem, c.stream, a);
+  a.staged = P.staged;
+  launch_coop(ilu_sweep_kernel<S, BACK>, P.grid_sweep, 32 * P.sweep_warps, P.sweep_smem, c.stream, a);
 }
 
 template <bool BACK>
@@ -659,14 +792,14 @@ void sweep_dispatch(Ctx &c, IluPlan &P, const double *in, double *out) {
 
 template <int RMAX, bool SMEM>
 void factor_launch(Ctx &c, IluPlan &P) {
-  auto kern = ilu_factor_kernel<RMAX, SMEM>;
-  const size_t smem = SMEM ? sizeof(double) * 3 * (size_t)P.B * P.B : 0;
-  const int grid = coop_grid(kern, 256, smem, P.grid_factor);
   FactorArgs a{};
-  a.sc = Sched{P.chunk, P.chunks, grid};
   a.B = P.B;
+  a.maxrow = P.maxrow;
+  a.maxupd = P.maxupd;
+  a.slot_ptr = P.slot_ptr[0];
+  a.meta = reinterpret_cast<const int4 *>(P.meta[0]);
+  a.deps = reinterpret_cast<const int2 *>(P.deps[0]);
   a.row = P.row;
-  a.col = P.col;
   a.diag = P.diag;
   a.upd_ptr = P.upd_ptr;
   a.upd = P.upd;
@@ -677,11 +810,11 @@ void factor_launch(Ctx &c, IluPlan &P) {
   a.abort = P.abort;
   a.err = c.derr;
   a.tag = (unsigned long long)(++P.epoch) << 32;
-  launch_coop(kern, grid, 256, smem, c.stream, a);
+  launch_coop(ilu_factor_kernel<RMAX, SMEM>, P.grid_factor, 256, SMEM ? P.factor_smem : 0, c.stream, a);
 }
 
 void factor_dispatch(Ctx &c, IluPlan &P) {
-  if (P.B <= kStageMaxB) {
+  if (P.staged) {
     if (P.B <= 32) factor_launch<1, true>(c, P);
     else factor_launch<2, true>(c, P);
     return;

@@ -112,8 +112,14 @@ struct IluPlan {
   unsigned long long *progress = nullptr;        // one counter per CTA of a sweep
   int *abort = nullptr;
   unsigned epoch = 0;
-  int grid_factor = 0, grid_sweep = 0, sweep_warps = 0, stage_doubles = 0;
-  size_t sweep_smem = 0;
+  int grid_factor = 0, grid_sweep = 0, sweep_warps = 0, staged = 0, ring = 0, maxrow = 0, maxupd = 0;
+  size_t sweep_smem = 0, factor_smem = 0;
+  // sweep schedules (forward, backward): per CTA the first position, per
+  // position (row, first entry, entry count) and the (owner<<22|slot, column)
+  // of each entry's dependency
+  int *slot_ptr[2] = {nullptr, nullptr};
+  int *meta[2] = {nullptr, nullptr};
+  int *deps[2] = {nullptr, nullptr};
 };
 
 struct Ctx {
