@@ -222,7 +222,7 @@ def max_over_ranks(world, value: float) -> float:
     return float(t.item())
 
 
-def make_context(w, form, device=0):
+def make_context(w, form, device=0, precision="fp64"):
     from mfem_euler2d_cpp_b200 import capi
 
     lib = capi.load()
@@ -230,7 +230,8 @@ def make_context(w, form, device=0):
         raise RuntimeError("eg_set_device failed")
     d = capi.simple_wave_desc(w["nx"], w["ny"], w["k"], w["alpha"])
     o = capi.default_opts(form=capi.FORM_HDG if form == "hdg" else capi.FORM_DG,
-                          precond=capi.PC_JACOBI if w["precond"] == "block-jacobi" else capi.PC_ILU0)
+                          precond=capi.PC_JACOBI if w["precond"] == "block-jacobi" else capi.PC_ILU0,
+                          precision=capi.PRECISION_MIXED if precision == "mixed" else capi.PRECISION_FP64)
     return capi.Context(d, o)
 
 
@@ -374,6 +375,33 @@ def run_ours(args, world, rank, local):
         std.close()
         ctxd.close()
 
+    # the same HDG workload in mixed precision (secondary line)
+    mixed = None
+    if not args.no_mixed:
+        ctxm = make_context(w, "hdg", local, precision="mixed")
+        stm = make_stepper(ctxm, w, W + K, "hdg")
+        extm = torch.cuda.ExternalStream(ctxm.stream_ptr())
+        for _ in range(W):
+            stm.next()
+        ctxm.lib.eg_profile_reset(ctxm.h)
+        ctxm.lib.eg_profile_enable(ctxm.h, 1)
+        mx_ms, mx_dev = timed_updates(ctxm, stm, K, world, extm)
+        mx_kry = timed_updates.krylov
+        mx_prof = {}
+        for i, name in enumerate(K_NAMES):
+            import ctypes as C
+
+            ms, cnt = C.c_double(), C.c_longlong()
+            ctxm.lib.eg_profile_query(ctxm.h, i, C.byref(ms), C.byref(cnt))
+            if cnt.value:
+                mx_prof[name] = round(ms.value / K, 3)
+        mx_ms = max_over_ranks(world, mx_ms)
+        mixed = {"value": mx_ms * 1e-3 / (K * world), "unit": "s", "ms_per_step": mx_ms / K,
+                 "mean_newton_device_s": mx_dev * 1e-3 / K, "precision": "mixed",
+                 "krylov_per_update": mx_kry / K, "kernel_ms_per_update": mx_prof}
+        stm.close()
+        ctxm.close()
+
     # the same HDG workload preconditioned by block ILU(0) (secondary line)
     ilu = None
     if not args.no_ilu:
@@ -487,6 +515,7 @@ def run_ours(args, world, rank, local):
         "clocks": clocks,
         "dg": dg,
         "ilu": ilu,
+        "mixed": mixed,
     }
     return line
 
@@ -532,6 +561,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--no-dg", action="store_true", help="skip the secondary DG-form measurement")
     ap.add_argument("--no-ilu", action="store_true", help="skip the secondary block-ILU(0) measurement")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-updates", type=int, default=12)
     args = ap.parse_args()

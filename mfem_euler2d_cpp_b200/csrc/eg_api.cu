@@ -230,9 +230,18 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
   out.setup = now_s() - t0;
   t0 = now_s();
   int count = 0;
+  // mixed precision: FP32 inner solve of the condensed system in FP64
+  // refinement (block Jacobi only; DG and block ILU(0) stay FP64)
+  const bool mixed = c.opts.precision == EG_PRECISION_MIXED && form == EG_FORM_HDG &&
+                     c.opts.precond == EG_PC_BLOCK_JACOBI;
   double res = 0.;
   try {
-    res = gmres(c, ops, rhs, x, tol, c.opts.max_krylov, refresh, &count, nullptr);
+    if (mixed) {
+      if (refresh) mixed_prepare(c);
+      res = schur_refine_mixed(c, rhs, x, refresh, tol, c.opts.max_krylov, rhs_norm, &count);
+    } else {
+      res = gmres(c, ops, rhs, x, tol, c.opts.max_krylov, refresh, &count, nullptr);
+    }
   } catch (const Failure &) {
     c.check_device_error();  // a preconditioner failure on the device explains the breakdown
     throw;
@@ -457,6 +466,8 @@ static void validate_opts(const eg_opts &o) {
   if (o.restart <= 0 || o.max_krylov <= 0) eg::fail(EG_ERR_INVALID, "Iteration limits must be positive");
   if (o.restart > eg::kMaxRestart) eg::fail(EG_ERR_INVALID, "restart above the supported maximum of 64");
   if (!(o.linear_tol > 0)) eg::fail(EG_ERR_INVALID, "linear tolerance must be positive");
+  if (o.precision != EG_PRECISION_FP64 && o.precision != EG_PRECISION_MIXED)
+    eg::fail(EG_ERR_INVALID, "Invalid precision");
 }
 
 int eg_create(const eg_desc *d, const eg_opts *o, eg_ctx **out) {

@@ -87,14 +87,25 @@ struct ProfScope {
   ~ProfScope();
 };
 
-// Operators used by the Krylov solver.
-struct LinearOps {
+// Operators used by the Krylov solver, on vectors of type T.
+template <class T>
+struct LinearOpsT {
   int N;
   const double *mtab;  // metric table (device)
   int period;          // metric period in entries
-  virtual void apply(Ctx &c, const double *x, double *y) = 0;
-  virtual void precondition(Ctx &c, const double *b, double *x) = 0;
-  virtual ~LinearOps() = default;
+  virtual void apply(Ctx &c, const T *x, T *y) = 0;
+  virtual void precondition(Ctx &c, const T *b, T *x) = 0;
+  virtual ~LinearOpsT() = default;
+};
+using LinearOps = LinearOpsT<double>;
+
+// Krylov workspace of one vector type: basis (R+1 columns, leading dimension
+// ld) and the work vectors of the solver.
+template <class T>
+struct KrylovBufs {
+  T *V, *w, *z, *res, *comb, *corr;
+  size_t ld;
+  int R;
 };
 
 // Block ILU(0) of one form (FixedBlockILU, src/block_ilu.cpp:10-109): fixed
@@ -173,6 +184,11 @@ struct Ctx {
   bool update_timer_open = false;
 
   IluPlan ilu[2];  // per form (EG_FORM_DG, EG_FORM_HDG)
+  // mixed precision: FP32 copies of X, of the Schur block-Jacobi inverses and
+  // of D, and the FP32 Krylov workspace of the inner Schur solve
+  float *Xf = nullptr, *pcf = nullptr, *Df = nullptr, *contribf = nullptr;
+  float *kfV = nullptr, *kfw = nullptr, *kfz = nullptr, *kfres = nullptr, *kfcomb = nullptr,
+        *kfcorr = nullptr, *kfx = nullptr, *kfrhs = nullptr;
 
   bool residual_ready = false;
   bool condensed = false;
@@ -214,6 +230,14 @@ void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, 
 // condensation; x = ILU^{-1} b.
 void ilu_refresh(Ctx &c, int form, bool factor);
 void launch_ilu_apply(Ctx &c, int form, const double *b, double *x);
+// ---- mixed precision (eg_mixed.cu) ----
+// FP32 copies of the condensed responses and of the factored Schur
+// block-Jacobi inverses (after eg_condense and the FP64 factor).
+void mixed_prepare(Ctx &c);
+// S x = rhs by FP64 iterative refinement around an FP32 inner GMRES; leaves
+// rhs - S x in c.kres and returns its weighted norm. *count = inner iterations.
+double schur_refine_mixed(Ctx &c, const double *rhs, double *x, bool zero_guess, double tol, int limit,
+                          double rhs_norm, int *count);
 // ---- launchers (eg_krylov.cu) ----
 // Weighted squared norm sum(metric * x * x) into dscal[slot] (device).
 void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot);
@@ -226,6 +250,10 @@ double cell_norm(Ctx &c, const double *x);
 // norm; sets *count. Throws Failure on breakdown / limit / non-finite.
 double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
              bool zero_guess, int *count, double *rhs_norm_out);
+// The same iteration on FP32 vectors from a zero guess; returns the residual
+// norm reached without requiring convergence (inner solve of mixed precision).
+double gmres_f32(Ctx &c, LinearOpsT<float> &ops, const KrylovBufs<float> &kb, const float *rhs, float *x,
+                 double tol, int limit, int *count);
 // ---- eg_api.cu ----
 // One accepted damped Newton update (src/stepper.cpp:129-228).
 void newton_update(Ctx &c, double residual_norm, double old_norm, eg_update_stats *st);

@@ -44,8 +44,9 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 constexpr int kChunk = 8;  // Krylov columns per register chunk
 
 // ---------------------------------------------------------- weighted norm
+template <class T>
 __global__ void __launch_bounds__(kRedThreads)
-    wnorm2_kernel(int N, const double *__restrict__ x, const double *__restrict__ mtab, int period,
+    wnorm2_kernel(int N, const T *__restrict__ x, const double *__restrict__ mtab, int period,
                   double *partials, unsigned *counter, double *out) {
   __shared__ double red[kRedThreads];
   __shared__ double mt[2 * EG_MAX_P];
@@ -53,7 +54,7 @@ __global__ void __launch_bounds__(kRedThreads)
   __syncthreads();
   double s = 0.;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const double v = x[i];
+    const double v = (double)x[i];
     s += mt[(i % period) >> 2] * v * v;
   }
   s = block_sum(s, red);
@@ -74,9 +75,10 @@ __global__ void __launch_bounds__(kRedThreads)
 // MODE 1: w -= V proj_in; proj = V^T (metric w)        (second pass)
 // MODE 2: w -= V proj_in; next = ||w||_metric         (norm)
 // proj results are added into the Hessenberg column (h(i,j) += proj_i).
-template <int MODE>
+// T is the storage type of the Krylov vectors; sums are formed in FP64.
+template <int MODE, class T>
 __global__ void __launch_bounds__(kRedThreads)
-    cgs_kernel(int N, double *__restrict__ w, const double *__restrict__ V, size_t ldv, int ncols,
+    cgs_kernel(int N, T *__restrict__ w, const T *__restrict__ V, size_t ldv, int ncols,
                const double *__restrict__ mtab, int period, double *partials, unsigned *counter,
                GmresCtl *ctl, int R) {
   __shared__ double red[kRedThreads];
@@ -92,10 +94,10 @@ __global__ void __launch_bounds__(kRedThreads)
     double s = 0.;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
       double comb = 0.;
-      for (int c = 0; c < ncols; ++c) comb += V[c * ldv + i] * pin[c];
-      const double v = w[i] - comb;
+      for (int c = 0; c < ncols; ++c) comb += (double)V[c * ldv + i] * pin[c];
+      const T v = (T)((double)w[i] - comb);
       w[i] = v;
-      s += mt[(i % period) >> 2] * v * v;
+      s += mt[(i % period) >> 2] * (double)v * (double)v;
     }
     s = block_sum(s, red);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
@@ -116,8 +118,8 @@ __global__ void __launch_bounds__(kRedThreads)
   if (MODE == 1) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
       double comb = 0.;
-      for (int c = 0; c < ncols; ++c) comb += V[c * ldv + i] * pin[c];
-      w[i] -= comb;
+      for (int c = 0; c < ncols; ++c) comb += (double)V[c * ldv + i] * pin[c];
+      w[i] = (T)((double)w[i] - comb);
     }
     // each thread re-reads only its own elements below: no grid barrier needed
   }
@@ -127,10 +129,10 @@ __global__ void __launch_bounds__(kRedThreads)
 #pragma unroll
     for (int k = 0; k < kChunk; ++k) acc[k] = 0.;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-      const double wm = mt[(i % period) >> 2] * w[i];
+      const double wm = mt[(i % period) >> 2] * (double)w[i];
 #pragma unroll
       for (int k = 0; k < kChunk; ++k)
-        if (k < nc) acc[k] += V[(c0 + k) * ldv + i] * wm;
+        if (k < nc) acc[k] += (double)V[(c0 + k) * ldv + i] * wm;
     }
     for (int k = 0; k < nc; ++k) {
       const double s = block_sum(acc[k], red);
@@ -152,13 +154,13 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 // V_{j+1} = w * (1/next) when next > 0 (src/linear.cpp:119-122)
-__global__ void normalize_kernel(int N, const double *__restrict__ w, double *__restrict__ vnext,
-                                 const GmresCtl *ctl) {
+template <class T>
+__global__ void normalize_kernel(int N, const T *__restrict__ w, T *__restrict__ vnext, const GmresCtl *ctl) {
   const double next = ctl->next;
   if (!(next > 0)) return;
   const double s = 1. / next;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-    vnext[i] = w[i] * s;
+    vnext[i] = (T)((double)w[i] * s);
 }
 
 // Givens update of Hessenberg column j and the convergence test
@@ -214,16 +216,17 @@ __global__ void cycle_init_kernel(GmresCtl *ctl, int R, double beta, double abs_
 }
 
 // out = V[:, 0:count] y (src/linear.cpp:145-146)
-__global__ void combine_kernel(int N, const double *__restrict__ V, size_t ldv,
-                               const GmresCtl *__restrict__ ctl, double *__restrict__ out) {
+template <class T>
+__global__ void combine_kernel(int N, const T *__restrict__ V, size_t ldv, const GmresCtl *__restrict__ ctl,
+                               T *__restrict__ out) {
   __shared__ double ys[kMaxRestart];
   const int count = ctl->count;
   for (int i = threadIdx.x; i < count; i += blockDim.x) ys[i] = ctl->y[i];
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     double s = 0.;
-    for (int c = 0; c < count; ++c) s += V[c * ldv + i] * ys[c];
-    out[i] = s;
+    for (int c = 0; c < count; ++c) s += (double)V[c * ldv + i] * ys[c];
+    out[i] = (T)s;
   }
 }
 
@@ -232,30 +235,45 @@ __global__ void axpby_kernel(int N, double a, const double *__restrict__ x, doub
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     out[i] = a * x[i] + b * y[i];
 }
-__global__ void scale_kernel(int N, double a, const double *__restrict__ x, double *__restrict__ out) {
+template <class T>
+__global__ void scale_kernel(int N, double a, const T *__restrict__ x, T *__restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-    out[i] = x[i] * a;
+    out[i] = (T)((double)x[i] * a);
 }
-__global__ void sub_kernel(int N, const double *__restrict__ x, const double *__restrict__ y,
-                           double *__restrict__ out) {
+template <class T>
+__global__ void sub_kernel(int N, const T *__restrict__ x, const T *__restrict__ y, T *__restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     out[i] = x[i] - y[i];
 }
-__global__ void add_kernel(int N, const double *__restrict__ x, double *__restrict__ y) {
+template <class T>
+__global__ void add_kernel(int N, const T *__restrict__ x, T *__restrict__ y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     y[i] += x[i];
 }
-__global__ void fill_kernel(int N, double v, double *__restrict__ out) {
+template <class T>
+__global__ void fill_kernel(int N, T v, T *__restrict__ out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) out[i] = v;
 }
 
 static int vec_grid(int N) { return std::max(1, std::min((N + 255) / 256, 148 * 16)); }
 
-void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot) {
+template <class T>
+void launch_wnorm2_t(Ctx &c, const T *x, int N, const double *mtab, int period, int slot) {
   ProfScope ps(c, EG_K_KRYLOV, 1);
-  wnorm2_kernel<<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, x, mtab, period, c.partials, c.counter,
-                                                          c.dscal + slot);
+  wnorm2_kernel<T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, x, mtab, period, c.partials, c.counter,
+                                                             c.dscal + slot);
   EG_CUDA(cudaGetLastError());
+}
+void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot) {
+  launch_wnorm2_t(c, x, N, mtab, period, slot);
+}
+template <class T>
+double wnorm_t(Ctx &c, const T *x, int N, const double *mtab, int period) {
+  launch_wnorm2_t(c, x, N, mtab, period, DS_NORM);
+  EG_CUDA(cudaMemcpyAsync(c.hscal + DS_NORM, c.dscal + DS_NORM, sizeof(double),
+                          cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  return std::sqrt(c.hscal[DS_NORM]);
 }
 double wnorm(Ctx &c, const double *x, int N, const double *mtab, int period) {
   launch_wnorm2(c, x, N, mtab, period, DS_NORM);
@@ -277,58 +295,65 @@ void launch_copy(Ctx &c, int N, const double *x, double *out) {
 }
 void launch_fill(Ctx &c, int N, double v, double *out) {
   ProfScope ps(c, EG_K_VECTOR, 1);
-  fill_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, v, out);
+  fill_kernel<double><<<vec_grid(N), 256, 0, c.stream>>>(N, v, out);
   EG_CUDA(cudaGetLastError());
 }
 
 // -------------------------------------------------------------------- GMRES
-double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
-             bool zero_guess, int *count, double *rhs_norm_out) {
-  c.ensure_krylov();
+// Weighted restarted CGS2 GMRES on vectors of type T (FP64 for the parity
+// path, FP32 for the inner solve of mixed precision); scalars, Hessenberg,
+// Givens and all sums are FP64.
+template <class T>
+double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs, T *x, double tol, int limit,
+               bool zero_guess, bool require_converged, int *count, double *rhs_norm_out) {
   const int N = ops.N;
-  const int R = std::min(N, c.kR);
-  const size_t ldv = (size_t)c.kN;
-  double *res = c.kres, *w = c.kw, *z = c.kz;
+  const int R = std::min(N, kb.R);
+  const size_t ldv = kb.ld;
+  T *res = kb.res, *w = kb.w, *z = kb.z, *V = kb.V;
   if (zero_guess) {
-    launch_fill(c, N, 0., x);
-    launch_copy(c, N, rhs, res);
+    {
+      ProfScope ps(c, EG_K_VECTOR, 1);
+      fill_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, T(0), x);
+      EG_CUDA(cudaGetLastError());
+    }
+    EG_CUDA(cudaMemcpyAsync(res, rhs, sizeof(T) * N, cudaMemcpyDeviceToDevice, c.stream));
   } else {
     ops.apply(c, x, w);
     ProfScope ps(c, EG_K_VECTOR, 1);
-    sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
+    sub_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
     EG_CUDA(cudaGetLastError());
   }
-  const double rhs_norm = wnorm(c, rhs, N, ops.mtab, ops.period);
+  const double rhs_norm = wnorm_t(c, rhs, N, ops.mtab, ops.period);
   if (rhs_norm_out) *rhs_norm_out = rhs_norm;
   *count = 0;
   if (rhs_norm == 0.) return 0.;
   int iterations = 0;
-  double residual_norm = wnorm(c, res, N, ops.mtab, ops.period);
+  double residual_norm = wnorm_t(c, res, N, ops.mtab, ops.period);
   while (iterations < limit) {
     const double beta = residual_norm;
     if (beta <= tol * rhs_norm) break;
     {
       ProfScope ps(c, EG_K_KRYLOV, 2);
-      scale_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, 1 / beta, res, c.V);
+      scale_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, 1 / beta, res, V);
       cycle_init_kernel<<<1, 256, 0, c.stream>>>(c.ctl, R, beta, tol * rhs_norm);
       EG_CUDA(cudaGetLastError());
     }
     for (int j = 0; j < R && iterations < limit; ++j) {
-      const double *vj = c.V + (size_t)j * ldv;
+      const T *vj = V + (size_t)j * ldv;
       ops.precondition(c, vj, z);
       ops.apply(c, z, w);
       const int nc = j + 1;
       {
-      ProfScope ps(c, EG_K_KRYLOV, 5);
-      cgs_kernel<0><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
-                                                              c.partials, c.counter, c.ctl, R);
-      cgs_kernel<1><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
-                                                              c.partials, c.counter, c.ctl, R);
-      cgs_kernel<2><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, c.V, ldv, nc, ops.mtab, ops.period,
-                                                              c.partials, c.counter, c.ctl, R);
-      normalize_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, w, c.V + (size_t)(j + 1) * ldv, c.ctl);
-      givens_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
-      EG_CUDA(cudaGetLastError());
+        ProfScope ps(c, EG_K_KRYLOV, 5);
+        cgs_kernel<0, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, ops.mtab, ops.period,
+                                                                   c.partials, c.counter, c.ctl, R);
+        cgs_kernel<1, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, ops.mtab, ops.period,
+                                                                   c.partials, c.counter, c.ctl, R);
+        cgs_kernel<2, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, ops.mtab, ops.period,
+                                                                   c.partials, c.counter, c.ctl, R);
+        normalize_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, w, V + (size_t)(j + 1) * ldv, c.ctl);
+        givens_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
+        EG_CUDA(cudaGetLastError());
       }
       EG_CUDA(cudaMemcpyAsync(&c.hctl->stop, &c.ctl->stop, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                               c.stream));
@@ -340,26 +365,39 @@ double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, i
     {
       ProfScope ps(c, EG_K_KRYLOV, 2);
       backsub_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
-      combine_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.V, ldv, c.ctl, c.kcomb);
+      combine_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, V, ldv, c.ctl, kb.comb);
       EG_CUDA(cudaGetLastError());
     }
-    ops.precondition(c, c.kcomb, c.kcorr);
+    ops.precondition(c, kb.comb, kb.corr);
     {
       ProfScope ps(c, EG_K_VECTOR, 1);
-      add_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, c.kcorr, x);
+      add_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, kb.corr, x);
     }
     ops.apply(c, x, w);
     {
       ProfScope ps(c, EG_K_VECTOR, 1);
-      sub_kernel<<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
+      sub_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
       EG_CUDA(cudaGetLastError());
     }
-    residual_norm = wnorm(c, res, N, ops.mtab, ops.period);
+    residual_norm = wnorm_t(c, res, N, ops.mtab, ops.period);
     if (!std::isfinite(residual_norm)) fail(EG_ERR_GMRES_NONFINITE, "Nonfinite GMRES residual");
   }
   *count = iterations;
-  if (!(residual_norm <= tol * rhs_norm)) fail(EG_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
+  if (require_converged && !(residual_norm <= tol * rhs_norm))
+    fail(EG_ERR_GMRES_LIMIT, "GMRES iteration limit reached");
   return residual_norm;
+}
+
+double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
+             bool zero_guess, int *count, double *rhs_norm_out) {
+  c.ensure_krylov();
+  const KrylovBufs<double> kb{c.V, c.kw, c.kz, c.kres, c.kcomb, c.kcorr, (size_t)c.kN, c.kR};
+  return gmres_t<double>(c, ops, kb, rhs, x, tol, limit, zero_guess, true, count, rhs_norm_out);
+}
+
+double gmres_f32(Ctx &c, LinearOpsT<float> &ops, const KrylovBufs<float> &kb, const float *rhs, float *x,
+                 double tol, int limit, int *count) {
+  return gmres_t<float>(c, ops, kb, rhs, x, tol, limit, true, false, count, nullptr);
 }
 
 }  // namespace eg

@@ -31,6 +31,7 @@ def main(argv=None):
     ap.add_argument("--op", choices=OPS, default="condense")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--precond", choices=sorted(PRECONDS), default="block-jacobi")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
     ap.add_argument("--form", choices=("dg", "hdg"), default=None,
                     help="form of the context (default: dg for dg_apply/dg_jacobi, hdg otherwise)")
     args = ap.parse_args(argv)
@@ -40,7 +41,8 @@ def main(argv=None):
     else:
         form = capi.FORM_DG if args.form == "dg" else capi.FORM_HDG
     d = capi.simple_wave_desc(args.nx, args.ny, args.k, args.alpha)
-    with capi.Context(d, capi.default_opts(form=form, precond=PRECONDS[args.precond])) as ctx:
+    prec = capi.PRECISION_MIXED if args.precision == "mixed" else capi.PRECISION_FP64
+    with capi.Context(d, capi.default_opts(form=form, precond=PRECONDS[args.precond], precision=prec)) as ctx:
         ctx.initial()
         rate = ctx.freeze(1e-3)
         dt = 0.24169426078821 / rate  # first SSP-DIRK3 stage at CFL 1
@@ -57,6 +59,7 @@ def main(argv=None):
         rng = np.random.default_rng(0)
         vb = rng.standard_normal(ctx.nu)
         vt = rng.standard_normal(ctx.nl)
+        out_counts = []
         lib.eg_profile_reset(ctx.h)
         lib.eg_profile_enable(ctx.h, 1)
         for _ in range(args.reps):
@@ -75,12 +78,15 @@ def main(argv=None):
             elif args.op == "residual":
                 ctx.residual()
             elif args.op == "linear_solve":
-                ctx.linear_solve(ctx.download("RHS"))
+                _, _, st = ctx.linear_solve(ctx.download("RHS"))
+                out_counts.append(st.count)
         names = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "recover",
                  "recovered_residual", "schur_jacobi", "pc_apply", "krylov", "freeze", "admissible",
                  "vector"]
         out = {"op": args.op, "nx": args.nx, "ny": args.ny, "k": args.k, "reps": args.reps,
-               "precond": args.precond}
+               "precond": args.precond, "precision": args.precision}
+        if out_counts:
+            out["krylov_counts"] = out_counts
         for i, name in enumerate(names):
             ms, cnt = C.c_double(), C.c_longlong()
             lib.eg_profile_query(ctx.h, i, C.byref(ms), C.byref(cnt))
