@@ -153,6 +153,105 @@ __global__ void __launch_bounds__(kRedThreads)
   }
 }
 
+// Register-resident CGS2 passes for up to NC basis columns: every element's
+// basis values are loaded once per pass and reused for the update of w and
+// the projection, each thread keeps several elements' loads in flight, and
+// sums are reduced with warp shuffles, then across the CTA, then in block
+// order by the last CTA (fixed grid: bitwise reproducible). Same MODE
+// semantics as cgs_kernel.
+constexpr int kCgsBlocks = 592;  // 4 CTAs per SM
+constexpr int kCgsThreads = 256;
+static_assert(kCgsBlocks * 24 <= kRedBlocks * (kMaxRestart + 1), "partials hold every CTA's column sums");
+
+template <int NC>
+__device__ __forceinline__ void cta_reduce_columns(double (&acc)[NC], int nc, double *red /* [8][NC] */,
+                                                   double *partials, int nblocks) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0 && k < nc) red[warp * NC + k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < nc) {
+    double t = 0.;
+    for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) t += red[wv * NC + threadIdx.x];
+    partials[(size_t)threadIdx.x * nblocks + blockIdx.x] = t;
+  }
+}
+
+template <int MODE, class T, int NC>
+__global__ void __launch_bounds__(kCgsThreads)
+    cgs_reg_kernel(int N, T *__restrict__ w, const T *__restrict__ V, size_t ldv, int ncols,
+                   const double *__restrict__ mtab, int period, double *partials, unsigned *counter,
+                   GmresCtl *ctl, int R) {
+  __shared__ double red[8 * NC];
+  __shared__ double mt[2 * EG_MAX_P];
+  __shared__ double pin[NC];
+  __shared__ double fin[kCgsThreads];
+  for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
+  if (MODE > 0)
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) pin[i] = ctl->proj[i];
+  __syncthreads();
+  const int j = ctl->j;
+  double acc[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc[k] = 0.;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    double v[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) v[k] = k < ncols ? (double)V[(size_t)k * ldv + i] : 0.;
+    const double m = mt[(i % period) >> 2];
+    double wi = (double)w[i];
+    if (MODE > 0) {
+      double comb = 0.;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) comb += v[k] * (k < ncols ? pin[k] : 0.);
+      const T wn = (T)(wi - comb);
+      w[i] = wn;
+      wi = (double)wn;
+    }
+    if (MODE == 2) {
+      acc[0] += m * wi * wi;
+    } else {
+      const double wm = m * wi;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) acc[k] += v[k] * wm;
+    }
+  }
+  const int nred = MODE == 2 ? 1 : ncols;
+  cta_reduce_columns<NC>(acc, nred, red, partials, gridDim.x);
+  if (last_block(counter)) {
+    for (int c = 0; c < nred; ++c) {
+      double t = 0.;
+      for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) t += partials[(size_t)c * gridDim.x + b];
+      fin[threadIdx.x] = t;
+      __syncthreads();
+      for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) fin[threadIdx.x] += fin[threadIdx.x + s];
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) {
+        const double tot = fin[0];
+        if (MODE == 2) {
+          const double next = sqrt(tot);
+          ctl->next = next;
+          ctl->inv_next = next > 0 ? 1. / next : 0.;
+          ctl->h[(j + 1) + (R + 1) * j] = next;
+        } else {
+          ctl->proj[c] = tot;
+          ctl->h[c + (R + 1) * j] += tot;
+        }
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) *counter = 0;
+  }
+}
+
 // V_{j+1} = w * (1/next) when next > 0 (src/linear.cpp:119-122)
 template <class T>
 __global__ void normalize_kernel(int N, const T *__restrict__ w, T *__restrict__ vnext, const GmresCtl *ctl) {
@@ -299,6 +398,36 @@ void launch_fill(Ctx &c, int N, double v, double *out) {
   EG_CUDA(cudaGetLastError());
 }
 
+// The three CGS2 passes of Arnoldi step j (src/linear.cpp:104-118).
+template <class T, int NC>
+void cgs_reg_passes(Ctx &c, int N, T *w, const T *V, size_t ldv, int nc, const double *mtab, int period, int R) {
+  cgs_reg_kernel<0, T, NC><<<kCgsBlocks, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                                     c.counter, c.ctl, R);
+  cgs_reg_kernel<1, T, NC><<<kCgsBlocks, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                                     c.counter, c.ctl, R);
+  cgs_reg_kernel<2, T, NC><<<kCgsBlocks, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                                     c.counter, c.ctl, R);
+}
+template <class T>
+void cgs_passes(Ctx &c, int N, T *w, const T *V, size_t ldv, int nc, const double *mtab, int period, int R) {
+  if (nc <= 4) {
+    cgs_reg_passes<T, 4>(c, N, w, V, ldv, nc, mtab, period, R);
+  } else if (nc <= 8) {
+    cgs_reg_passes<T, 8>(c, N, w, V, ldv, nc, mtab, period, R);
+  } else if (nc <= 16) {
+    cgs_reg_passes<T, 16>(c, N, w, V, ldv, nc, mtab, period, R);
+  } else if (nc <= 24) {
+    cgs_reg_passes<T, 24>(c, N, w, V, ldv, nc, mtab, period, R);
+  } else {
+    cgs_kernel<0, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                               c.counter, c.ctl, R);
+    cgs_kernel<1, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                               c.counter, c.ctl, R);
+    cgs_kernel<2, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                               c.counter, c.ctl, R);
+  }
+}
+
 // -------------------------------------------------------------------- GMRES
 // Weighted restarted CGS2 GMRES on vectors of type T (FP64 for the parity
 // path, FP32 for the inner solve of mixed precision); scalars, Hessenberg,
@@ -345,12 +474,7 @@ double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs
       const int nc = j + 1;
       {
         ProfScope ps(c, EG_K_KRYLOV, 5);
-        cgs_kernel<0, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, ops.mtab, ops.period,
-                                                                   c.partials, c.counter, c.ctl, R);
-        cgs_kernel<1, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, ops.mtab, ops.period,
-                                                                   c.partials, c.counter, c.ctl, R);
-        cgs_kernel<2, T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, w, V, ldv, nc, ops.mtab, ops.period,
-                                                                   c.partials, c.counter, c.ctl, R);
+        cgs_passes<T>(c, N, w, V, ldv, nc, ops.mtab, ops.period, R);
         normalize_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, w, V + (size_t)(j + 1) * ldv, c.ctl);
         givens_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
         EG_CUDA(cudaGetLastError());
