@@ -283,6 +283,79 @@ typedef struct eg_stepper eg_stepper;
 int eg_stepper_create(eg_ctx *ctx, const eg_run_opts *ro, eg_stepper **out);
 int eg_stepper_next(eg_stepper *s, eg_update_stats *st);
 void eg_stepper_destroy(eg_stepper *s);
+/* After eg_stepper_next returned -1: final time, step count, L2 errors against
+ * the exact wave (Problem::Errors, src/problem.cpp:704) and the conservation
+ * drift of the final state (src/stepper.cpp:255-258). The update counters of
+ * res are left zero (the caller counts its eg_stepper_next calls). */
+int eg_stepper_finish(eg_stepper *s, eg_run_result *res);
+
+/* ------------------------------------- many instances: batch and serving */
+/* Neither has a counterpart in the reference, whose driver runs one problem
+ * per process. Every instance is an eg_ctx with its own CUDA stream; host
+ * worker threads advance the instances through the calls above, so the
+ * Newton updates of different instances overlap on the GPU. Each instance's
+ * kernels and reductions are the single-instance ones, so every result is
+ * bitwise the one the instance gives when run alone. */
+
+/* A fixed set of instances run to completion together (uneven nx, ny, k). */
+typedef struct eg_batch eg_batch;
+typedef struct eg_batch_stats {
+  double seconds;          /* wall time of eg_batch_run */
+  long long updates;       /* accepted Newton updates over all instances */
+  int failed;              /* instances whose run returned an error */
+} eg_batch_stats;
+/* count instances: descs[i] with opts[i], on `device`. */
+int eg_batch_create(int count, const eg_desc *descs, const eg_opts *opts, int device, eg_batch **out);
+/* Runs every instance through the schedule ro on `threads` host workers. */
+int eg_batch_run(eg_batch *b, const eg_run_opts *ro, int threads, eg_batch_stats *st);
+/* Per-instance outcome: status, updates and the final errors/drift. */
+int eg_batch_result(const eg_batch *b, int i, int *status, eg_run_result *res);
+/* The instance's context (its final state is EG_SLOT_U). */
+eg_ctx *eg_batch_context(eg_batch *b, int i);
+void eg_batch_destroy(eg_batch *b);
+
+/* A request loop: time-advance requests are submitted while others run;
+ * a request is admitted when a worker is free and its device memory fits the
+ * budget beside the requests already resident (first come, first served). */
+typedef struct eg_server eg_server;
+typedef struct eg_server_opts {
+  int device;
+  int workers;              /* concurrent requests on the GPU */
+  long long budget_bytes;   /* device memory budget of resident requests */
+  int keep_contexts;        /* reuse finished contexts of the same shape */
+  int keep_states;          /* copy each final state to host memory (eg_server_state) */
+} eg_server_opts;
+typedef struct eg_request {
+  int nx, ny, k;
+  double alpha_deg;
+  int steps, newton_steps;  /* SSP-DIRK3 steps; updates per stage (<= 0: converge) */
+  double cfl;
+  int form, precond, precision;
+} eg_request;
+typedef struct eg_request_result {
+  int status;               /* EG_OK or the failing call's status */
+  int updates;
+  double submit_s, start_s, finish_s;   /* server clock, seconds */
+  double final_time, errors[4], drift;
+  long long bytes;          /* device bytes charged against the budget */
+} eg_request_result;
+typedef struct eg_server_stats {
+  long long completed, failed;
+  long long peak_bytes;     /* largest sum of resident request bytes */
+  int peak_running;         /* largest number of requests on the GPU at once */
+} eg_server_stats;
+int eg_server_create(const eg_server_opts *o, eg_server **out);
+/* Queues a request; *id identifies it. Never blocks on the GPU. */
+int eg_server_submit(eg_server *s, const eg_request *r, long long *id);
+/* EG_OK when the request has finished (res filled), -1 while pending. */
+int eg_server_poll(eg_server *s, long long id, eg_request_result *res);
+/* Copies the final state (nx*ny*4(k+1)^2 doubles) of a finished request. */
+int eg_server_state(eg_server *s, long long id, double *u);
+/* Blocks until every submitted request has finished. */
+int eg_server_drain(eg_server *s, eg_server_stats *st);
+/* Seconds on the server clock (the time base of eg_request_result). */
+double eg_server_clock(const eg_server *s);
+void eg_server_destroy(eg_server *s);
 
 /* ------------------------------------------------- allocation-free entry */
 /* CellNorm of a body vector without any device allocation. This entry point

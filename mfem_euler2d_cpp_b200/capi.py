@@ -102,6 +102,32 @@ class RunResult(C.Structure):
     ]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("updates", C.c_longlong), ("failed", C.c_int)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("workers", C.c_int), ("budget_bytes", C.c_longlong),
+                ("keep_contexts", C.c_int), ("keep_states", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("k", C.c_int), ("alpha_deg", C.c_double),
+                ("steps", C.c_int), ("newton_steps", C.c_int), ("cfl", C.c_double),
+                ("form", C.c_int), ("precond", C.c_int), ("precision", C.c_int)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("updates", C.c_int), ("submit_s", C.c_double), ("start_s", C.c_double),
+                ("finish_s", C.c_double), ("final_time", C.c_double), ("errors", C.c_double * 4),
+                ("drift", C.c_double), ("bytes", C.c_longlong)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("failed", C.c_longlong), ("peak_bytes", C.c_longlong),
+                ("peak_running", C.c_int)]
+
+
 _lib = None
 _DP = C.POINTER(C.c_double)
 
@@ -160,6 +186,19 @@ def load() -> C.CDLL:
         "eg_stepper_create": (C.c_int, [vp, C.POINTER(RunOpts), C.POINTER(vp)]),
         "eg_stepper_next": (C.c_int, [vp, C.POINTER(UpdateStats)]),
         "eg_stepper_destroy": (None, [vp]),
+        "eg_stepper_finish": (C.c_int, [vp, C.POINTER(RunResult)]),
+        "eg_batch_create": (C.c_int, [C.c_int, C.POINTER(Desc), C.POINTER(Opts), C.c_int, C.POINTER(vp)]),
+        "eg_batch_run": (C.c_int, [vp, C.POINTER(RunOpts), C.c_int, C.POINTER(BatchStats)]),
+        "eg_batch_result": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(RunResult)]),
+        "eg_batch_context": (vp, [vp, C.c_int]),
+        "eg_batch_destroy": (None, [vp]),
+        "eg_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(vp)]),
+        "eg_server_submit": (C.c_int, [vp, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+        "eg_server_poll": (C.c_int, [vp, C.c_longlong, C.POINTER(RequestResult)]),
+        "eg_server_state": (C.c_int, [vp, C.c_longlong, _DP]),
+        "eg_server_drain": (C.c_int, [vp, C.POINTER(ServerStats)]),
+        "eg_server_clock": (C.c_double, [vp]),
+        "eg_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -387,3 +426,105 @@ def declared_symbols(header: Path = HEADER_PATH) -> list[str]:
     text = header.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(eg_[a-z0-9_]+)\s*\(", text)))
+
+
+class Batch:
+    """Independent instances run to completion together (eg_batch_*): one
+    context and CUDA stream per instance, `threads` host workers."""
+
+    def __init__(self, descs: list, opts: list, device: int = 0):
+        self.lib = load()
+        n = len(descs)
+        da, oa = (Desc * n)(*descs), (Opts * n)(*opts)
+        h = C.c_void_p()
+        rc = self.lib.eg_batch_create(n, da, oa, device, C.byref(h))
+        if rc != OK:
+            raise EngineError(rc, (self.lib.eg_last_error(None) or b"").decode())
+        self.h, self.n = h, n
+
+    def run(self, ro: RunOpts, threads: int = 16, check: bool = True) -> BatchStats:
+        """Runs every instance; with check=False failures are only counted
+        (per-instance statuses via result())."""
+        st = BatchStats()
+        rc = self.lib.eg_batch_run(self.h, C.byref(ro), threads, C.byref(st))
+        if rc != OK and check:
+            raise EngineError(rc, self.lib.eg_status_string(rc).decode())
+        return st
+
+    def result(self, i: int) -> tuple[int, RunResult]:
+        status, res = C.c_int(), RunResult()
+        self.lib.eg_batch_result(self.h, i, C.byref(status), C.byref(res))
+        return status.value, res
+
+    def state(self, i: int, nu: int) -> np.ndarray:
+        out = np.empty(nu)
+        ctx = self.lib.eg_batch_context(self.h, i)
+        rc = self.lib.eg_download(ctx, SLOT["U"], _ptr(out))
+        if rc != OK:
+            raise EngineError(rc, self.lib.eg_status_string(rc).decode())
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eg_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Server:
+    """Request loop with admission against a device-memory budget (eg_server_*)."""
+
+    def __init__(self, workers: int = 8, budget_bytes: int = 120 << 30, device: int = 0,
+                 keep_contexts: bool = True, keep_states: bool = False):
+        self.lib = load()
+        o = ServerOpts(device, workers, budget_bytes, int(keep_contexts), int(keep_states))
+        h = C.c_void_p()
+        rc = self.lib.eg_server_create(C.byref(o), C.byref(h))
+        if rc != OK:
+            raise EngineError(rc, self.lib.eg_status_string(rc).decode())
+        self.h = h
+
+    def submit(self, nx, ny, k, alpha_deg, steps, newton_steps=3, cfl=1.0, form=FORM_HDG, precond=PC_JACOBI,
+               precision=PRECISION_FP64) -> int:
+        r = Request(nx, ny, k, alpha_deg, steps, newton_steps, cfl, form, precond, precision)
+        rid = C.c_longlong()
+        rc = self.lib.eg_server_submit(self.h, C.byref(r), C.byref(rid))
+        if rc != OK:
+            raise EngineError(rc, self.lib.eg_status_string(rc).decode())
+        return rid.value
+
+    def poll(self, rid: int) -> RequestResult | None:
+        res = RequestResult()
+        rc = self.lib.eg_server_poll(self.h, rid, C.byref(res))
+        return res if rc == OK else None
+
+    def state(self, rid: int, nu: int) -> np.ndarray:
+        out = np.empty(nu)
+        rc = self.lib.eg_server_state(self.h, rid, _ptr(out))
+        if rc != OK:
+            raise EngineError(rc, "no stored state for this request")
+        return out
+
+    def drain(self) -> ServerStats:
+        st = ServerStats()
+        self.lib.eg_server_drain(self.h, C.byref(st))
+        return st
+
+    def clock(self) -> float:
+        return float(self.lib.eg_server_clock(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eg_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -184,6 +184,7 @@ struct Ctx {
   bool update_timer_open = false;
 
   IluPlan ilu[2];  // per form (EG_FORM_DG, EG_FORM_HDG)
+  double *step_bufs = nullptr;  // time loop: step state, stage base, 4 slopes (6 nu), reused
   // mixed precision: FP32 copies of X, of the Schur block-Jacobi inverses and
   // of D, and the FP32 Krylov workspace of the inner Schur solve
   float *Xf = nullptr, *pcf = nullptr, *Df = nullptr, *contribf = nullptr;

@@ -73,8 +73,10 @@ struct Stepper {
   }
 
   void begin() {
+    if (!c.step_bufs) c.step_bufs = c.alloc_n<double>((size_t)6 * c.nu);  // kept for later schedules
+    int slot = 0;
     for (double **v : {&step_state, &stage_base, &slope[0], &slope[1], &slope[2], &slope[3]}) {
-      *v = c.alloc_n<double>(c.nu);
+      *v = c.step_bufs + (size_t)(slot++) * c.nu;
       EG_CUDA(cudaMemsetAsync(*v, 0, sizeof(double) * c.nu, c.stream));
     }
     std::vector<double> u;
@@ -261,6 +263,26 @@ int eg_stepper_next(eg_stepper *s, eg_update_stats *st) {
 }
 
 void eg_stepper_destroy(eg_stepper *s) { delete s; }
+
+int eg_stepper_finish(eg_stepper *s, eg_run_result *res) {
+  if (!s || !res) return EG_ERR_INVALID;
+  eg::Stepper &st = s->s;
+  eg::Ctx &c = st.c;
+  return guard_run(c, [&] {
+    if (!st.done) eg::fail(EG_ERR_INVALID, "schedule not finished");
+    eg_run_result out{};
+    out.final_time = st.time;
+    out.time_steps = st.step;
+    std::vector<double> u(c.nu);
+    EG_CUDA(cudaMemcpyAsync(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    eg::host::errors(c.desc, u.data(), st.time, out.errors);
+    double fin[4];
+    eg::host::integral(c.desc, u.data(), fin);
+    for (int k = 0; k < 4; ++k) out.drift = std::max(out.drift, std::abs(fin[k] - st.initial_integral[k]));
+    *res = out;
+  });
+}
 
 int eg_run(eg_ctx *ctx, const eg_run_opts *ro, eg_run_result *res) {
   if (!ctx || !ro) return EG_ERR_INVALID;
