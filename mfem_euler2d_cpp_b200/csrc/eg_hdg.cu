@@ -681,6 +681,231 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
   }
 }
 
+// ------------------------------------------- condensation for k >= 5 (DMMA)
+// The cell system [A | B | r_e] (m x (m + 4t + 1)) does not fit on chip for
+// k >= 5, so it lives in a per-CTA slab of global memory (L2-resident) and is
+// reduced by blocked Gauss-Jordan with virtual partial pivoting in panels of
+// GjgCfg::NB columns:
+//  1. the panel's columns are staged in shared memory and its pivots chosen
+//     column by column exactly as row partial pivoting on the eliminated
+//     column would (largest magnitude among rows not yet used, first index on
+//     ties: the pivots of LUFactors::Factor, src/condensation.cpp:136-140);
+//  2. T = the panel's pivot rows and top = T^-1 W[pivot rows, trailing];
+//  3. one rank-NB update W[r, trailing] -= a_r top on the FP64 tensor cores
+//     (mma.sync m8n8k4), with a_r the row's panel entries, and T_r - e_r for
+//     the panel's own pivot rows, which turns them into the rows of top.
+// After the last panel the right-hand-side columns hold X = A^-1 B and
+// y = A^-1 r_e in pivot order and are written to XY in unknown order.
+template <int Q>
+struct GjgCfg {
+  static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, NC = M + NR;
+  static constexpr int NB = 16;                      // panel width
+  static constexpr int NPAN = (M + NB - 1) / NB;
+  static constexpr int MT = (M + 7) / 8;            // 8-row tiles
+  static constexpr size_t SMEM = sizeof(double) * ((size_t)2 * NB * M + (size_t)NB * NC + 2 * NB * NB) +
+                                 sizeof(int) * (size_t)(3 * M + NB);
+};
+
+template <int Q>
+__global__ void __launch_bounds__(256, 1)
+    condense_gjg_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                        const double *__restrict__ r, double *XY, double *Cb, double *sf, double *contrib,
+                        double *panels, double *work, int *err) {
+  using C = GjgCfg<Q>;
+  constexpr int M = C::M, NR = C::NR, NC = C::NC, NB = C::NB;
+  __shared__ CondenseShared<Q> sh;
+  __shared__ int sing;
+  __shared__ double pivval;
+  extern __shared__ __align__(16) double dyn[];
+  double *P0 = dyn;                          // original panel columns  [NB][M]
+  double *Pw = P0 + (size_t)NB * M;          // working panel columns   [NB][M]
+  double *top = Pw + (size_t)NB * M;         // [NB][NC] (trailing width)
+  double *Tm = top + (size_t)NB * NC;        // [NB][2NB] augmented [T | I], row-major
+  int *used = reinterpret_cast<int *>(Tm + 2 * NB * NB);
+  int *pidx = used + M;                      // panel index of a pivot row of this panel, else -1
+  int *piv = pidx + M;                       // pivot row of every column
+  int *prow = piv + M;                       // pivot rows of this panel
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  double *W = work + (size_t)blockIdx.x * M * NC;  // column-major, ld M
+  load_tables<Q>(sh.st, tab);
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    condense_build<Q>(sh, g, fz, u, r, Cb, sf, W, W + (size_t)M * M, e, M);
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+      used[i] = 0;
+      pidx[i] = -1;
+    }
+    if (threadIdx.x == 0) sing = 0;
+    __syncthreads();
+    for (int pan = 0; pan < C::NPAN; ++pan) {
+      const int c0 = pan * NB, nb = min(NB, M - c0), cs = c0 + nb, ntr = NC - cs;
+      // 1. stage the panel; choose its pivots on a working copy
+      for (int o = threadIdx.x; o < NB * M; o += blockDim.x) {
+        const int j = o / M, rr = o % M;
+        const double v = j < nb ? W[(size_t)(c0 + j) * M + rr] : 0.;
+        P0[o] = v;
+        Pw[o] = v;
+      }
+      __syncthreads();
+      for (int j = 0; j < nb; ++j) {
+        if (warp == 0) {
+          double best = -1.;
+          int bi = M;
+          for (int rr = lane; rr < M; rr += 32) {
+            if (used[rr]) continue;
+            const double v = fabs(Pw[(size_t)j * M + rr]);
+            if (v > best) {
+              best = v;
+              bi = rr;
+            }
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            const double ob = __shfl_down_sync(0xffffffffu, best, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (ob > best || (ob == best && oi < bi)) {
+              best = ob;
+              bi = oi;
+            }
+          }
+          if (lane == 0) {
+            const double pv = bi < M ? Pw[(size_t)j * M + bi] : 0.;  // an all-NaN column is singular
+            if (!(fabs(pv) > 0.)) {
+              sing = 1;
+              bi = 0;
+            }
+            pivval = pv;
+            prow[j] = bi;
+            piv[c0 + j] = bi;
+            used[bi] = 1;
+            pidx[bi] = j;
+          }
+        }
+        __syncthreads();
+        if (sing) break;
+        const int pr = prow[j];
+        const double inv = 1.0 / pivval;
+        const int rest = nb - j - 1;
+        for (int o = threadIdx.x; o < rest * M; o += blockDim.x) {
+          const int jj = j + 1 + o / M, rr = o % M;
+          if (rr != pr) Pw[(size_t)jj * M + rr] -= Pw[(size_t)j * M + rr] * inv * Pw[(size_t)jj * M + pr];
+        }
+        __syncthreads();
+      }
+      if (sing) break;
+      // 2. T^-1 by Gauss-Jordan with partial pivoting on [T | I] (nb x 2nb)
+      for (int o = threadIdx.x; o < NB * 2 * NB; o += blockDim.x) {
+        const int i = o / (2 * NB), k = o % (2 * NB);
+        double v = 0.;
+        if (i < nb && k < nb) v = P0[(size_t)k * M + prow[i]];
+        else if (k >= NB && k - NB == i) v = 1.;
+        else if (i >= nb && k == i) v = 1.;  // identity padding of a partial panel
+        Tm[o] = v;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        for (int j = 0; j < NB; ++j) {
+          // pivot among rows j..NB-1 of column j
+          double best = -1.;
+          int bi = j;
+          for (int i = j; i < NB; ++i) {
+            const double v = fabs(Tm[i * 2 * NB + j]);
+            if (v > best) {
+              best = v;
+              bi = i;
+            }
+          }
+          const double pv = Tm[bi * 2 * NB + j];
+          __syncwarp();
+          if (bi != j) {  // swap rows j and bi (lane = column)
+            const double a0 = Tm[j * 2 * NB + lane], b0 = Tm[bi * 2 * NB + lane];
+            __syncwarp();
+            Tm[j * 2 * NB + lane] = b0;
+            Tm[bi * 2 * NB + lane] = a0;
+          }
+          __syncwarp();
+          const double ip = 1.0 / pv;
+          Tm[j * 2 * NB + lane] *= ip;
+          __syncwarp();
+          double f[NB];
+#pragma unroll
+          for (int i = 0; i < NB; ++i) f[i] = Tm[i * 2 * NB + j];
+          __syncwarp();
+#pragma unroll
+          for (int i = 0; i < NB; ++i)
+            if (i != j) Tm[i * 2 * NB + lane] -= f[i] * Tm[j * 2 * NB + lane];
+          __syncwarp();
+        }
+      }
+      // top = T^-1 W[prow, trailing]: gather the pivot rows, then transform in place
+      for (int o = threadIdx.x; o < NB * ntr; o += blockDim.x) {
+        const int k = o / ntr, c = o % ntr;
+        top[(size_t)k * NC + c] = k < nb ? W[(size_t)(cs + c) * M + prow[k]] : 0.;
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < ntr; c += blockDim.x) {
+        double wv[NB], out[NB];
+#pragma unroll
+        for (int k = 0; k < NB; ++k) wv[k] = top[(size_t)k * NC + c];
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+          double s = 0.;
+#pragma unroll
+          for (int k = 0; k < NB; ++k) s += Tm[i * 2 * NB + NB + k] * wv[k];
+          out[i] = s;
+        }
+#pragma unroll
+        for (int i = 0; i < NB; ++i) top[(size_t)i * NC + c] = i < nb ? out[i] : 0.;
+      }
+      __syncthreads();
+      // 3. rank-NB update of the trailing columns on the tensor cores
+      const int ntile_c = (ntr + 7) / 8;
+      for (int ct = warp; ct < ntile_c; ct += nwarps) {
+        double bf[NB / 4];
+#pragma unroll
+        for (int ks = 0; ks < NB / 4; ++ks) {
+          const int cc = ct * 8 + gq;
+          bf[ks] = cc < ntr ? top[(size_t)(4 * ks + tq) * NC + cc] : 0.;
+        }
+        const int col0 = cs + ct * 8 + 2 * tq;
+        for (int rt = 0; rt < C::MT; ++rt) {
+          const int ra = rt * 8 + gq;  // row of this lane's A fragment and C values
+          double c0v = 0., c1v = 0.;
+          const bool rok = ra < M;
+          if (rok && col0 < NC) c0v = W[(size_t)col0 * M + ra];
+          if (rok && col0 + 1 < NC) c1v = W[(size_t)(col0 + 1) * M + ra];
+          const int pi = rok ? pidx[ra] : -1;
+#pragma unroll
+          for (int ks = 0; ks < NB / 4; ++ks) {
+            const int k = 4 * ks + tq;
+            double a = rok ? P0[(size_t)k * M + ra] : 0.;
+            if (pi == k) a -= 1.;
+            dmma_m8n8k4(c0v, c1v, -a, bf[ks]);
+          }
+          if (rok && col0 < NC) W[(size_t)col0 * M + ra] = c0v;
+          if (rok && col0 + 1 < NC) W[(size_t)(col0 + 1) * M + ra] = c1v;
+        }
+      }
+      __syncthreads();  // every warp has finished reading pidx for this panel
+      for (int j = threadIdx.x; j < nb; j += blockDim.x) pidx[prow[j]] = -1;
+      __syncthreads();
+    }
+    if (sing) {
+      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
+      continue;
+    }
+    // right-hand sides back to unknown order: X(j, c) = W(piv[j], M + c)
+    double *R = XY + (size_t)e * M * NR;
+    for (int o = threadIdx.x; o < M * NR; o += blockDim.x) {
+      const int c = o / M, j = o % M;
+      R[o] = W[(size_t)(M + c) * M + piv[j]];
+    }
+    __syncthreads();
+    condense_epilogue<Q>(sh, R, false, XY, contrib, panels, e);
+  }
+}
+
 // -------------------------------------------------- Schur action / recovery
 // Per cell: gather the 4t trace values, mid = X_e v_e (GEMV streaming X once),
 // then either restrict with C (Schur action, src/operators.cpp:166-178) or
@@ -867,6 +1092,20 @@ static void launch_condense_gj(Ctx &c, const double *u, const double *r) {
                                             c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
 }
 
+template <int Q>
+static void launch_condense_gjg(Ctx &c, const double *u, const double *r) {
+  using C = GjgCfg<Q>;
+  auto kern = condense_gjg_kernel<Q>;
+  EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
+  const int grid = std::min(c.n, sm_count_hdg());
+  if (c.work_gj == nullptr || c.work_gj_slots < grid) {
+    c.work_gj = c.alloc_n<double>((size_t)grid * C::M * C::NC);
+    c.work_gj_slots = grid;
+  }
+  kern<<<grid, 256, C::SMEM, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, r, c.XY,
+                                          c.Cb, c.sf, c.contrib, c.panels, c.work_gj, c.derr);
+}
+
 void launch_condense(Ctx &c, const double *u, const double *r) {
   c.ensure_hdg();
   const int grid = condense_grid(c);
@@ -877,6 +1116,10 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
     case 3: launch_condense_gj<3, 2, 2, 4>(c, u, r); break;
     case 4: launch_condense_gj<4, 2, 4, 2>(c, u, r); break;
     case 5: launch_condense_gj<5, 2, 4, 1>(c, u, r); break;
+    case 6: launch_condense_gjg<6>(c, u, r); break;
+    case 7: launch_condense_gjg<7>(c, u, r); break;
+    case 8: launch_condense_gjg<8>(c, u, r); break;
+    case 9: launch_condense_gjg<9>(c, u, r); break;
     default:
       EG_DISPATCH_Q(c.q, {
         constexpr size_t dyn = condense_dyn_bytes<Q>();

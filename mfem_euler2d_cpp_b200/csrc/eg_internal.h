@@ -161,6 +161,8 @@ struct Ctx {
   double *rhs = nullptr, *lam = nullptr, *tmp_trace = nullptr;  // nl
   double *work_cell = nullptr;  // global LU workspace for large cells
   int work_slots = 0;
+  double *work_gj = nullptr;    // k >= 5 condensation: one m x (m + 4t + 1) slab per CTA
+  int work_gj_slots = 0;
   // preconditioners (factored in place): DG n blocks m x m, HDG nf blocks t x t
   double *pc_dg = nullptr, *pc_hdg = nullptr;
   int *piv_dg = nullptr, *piv_hdg = nullptr;
