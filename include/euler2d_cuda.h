@@ -172,6 +172,10 @@ const char *eg_last_error(const eg_ctx *ctx);
 const char *eg_status_string(int status);
 /* cudaStream_t of the context, as void*. */
 void *eg_stream(eg_ctx *ctx);
+/* Re-describe a context for another problem of the same nx, ny and k (angle,
+ * box, gas, tables): the device buffers are kept, the state must be set anew.
+ * No counterpart in the reference (one Problem per run). */
+int eg_set_desc(eg_ctx *ctx, const eg_desc *d);
 /* Change solver options between updates (form, preconditioner, tolerance). */
 int eg_set_opts(eg_ctx *ctx, const eg_opts *o);
 /* Sizes: n, p, m, t, nf, nu, nl. */

@@ -372,6 +372,36 @@ void newton_update(Ctx &c, double residual_norm, double old_norm, eg_update_stat
   if (st) *st = s;
 }
 
+// Geometry and tables of the description (tab: [tdx][tdy][fb][w][inv_mass]
+// [mass][ew]; dual-norm metric tables), uploaded in stream order.
+void upload_desc(Ctx &c, const eg_desc &d) {
+  c.desc = d;
+  c.geo = Geo{d.nx, d.ny, c.n, c.nf, d.hx, d.hy, d.area, c.geo.dt, d.gamma, d.gamma - 1., d.safety};
+  const int q = c.q, p = c.p;
+  std::vector<double> tab(tab_size(q));
+  for (int i = 0; i < p; ++i) {
+    tab[i] = d.tensor_dx[i];
+    tab[p + i] = d.tensor_dy[i];
+    tab[6 * p + i] = d.w[i];
+    tab[7 * p + i] = d.inv_mass[i];
+    tab[8 * p + i] = d.mass[i];
+  }
+  for (int i = 0; i < 4 * p; ++i) tab[2 * p + i] = d.face_basis[i];
+  for (int j = 0; j < q; ++j) tab[9 * p + j] = d.ew[j];
+  std::vector<double> mdg(p), mhdg(2 * q);
+  for (int i = 0; i < p; ++i) mdg[i] = d.area * d.mass[i];
+  for (int j = 0; j < q; ++j) {
+    mhdg[j] = d.hy / d.ew[j];
+    mhdg[q + j] = d.hx / d.ew[j];
+  }
+  EG_CUDA(cudaMemcpyAsync(c.tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c.stream));
+  EG_CUDA(cudaMemcpyAsync(c.mtab_dg, mdg.data(), sizeof(double) * p, cudaMemcpyHostToDevice, c.stream));
+  EG_CUDA(cudaMemcpyAsync(c.mtab_hdg, mhdg.data(), sizeof(double) * 2 * q, cudaMemcpyHostToDevice, c.stream));
+  c.sync();  // the host tables are local
+  c.residual_ready = false;
+  c.condensed = false;
+}
+
 static double *slot_ptr(Ctx &c, int slot, size_t &count) {
   switch (slot) {
     case EG_SLOT_U: count = c.nu; return c.u;
@@ -495,50 +525,30 @@ int eg_create(const eg_desc *d, const eg_opts *o, eg_ctx **out) {
     for (int i = 0; i < c.p; ++i)
       if (d->tensor_node[i] != i)
         eg::fail(EG_ERR_INVALID, "native node order must be lexicographic (x fastest)");
-    c.geo = eg::Geo{d->nx, d->ny, c.n, c.nf, d->hx, d->hy, d->area, 0., d->gamma, d->gamma - 1., d->safety};
     EG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     EG_CUDA(cudaEventCreate(&c.ev0));
     EG_CUDA(cudaEventCreate(&c.ev1));
-    // tables: [tdx][tdy][fb][w][inv_mass][mass][ew]
-    const int q = c.q, p = c.p;
-    std::vector<double> tab(eg::tab_size(q));
-    for (int i = 0; i < p; ++i) {
-      tab[i] = d->tensor_dx[i];
-      tab[p + i] = d->tensor_dy[i];
-      tab[6 * p + i] = d->w[i];
-      tab[7 * p + i] = d->inv_mass[i];
-      tab[8 * p + i] = d->mass[i];
-    }
-    for (int i = 0; i < 4 * p; ++i) tab[2 * p + i] = d->face_basis[i];
-    for (int j = 0; j < q; ++j) tab[9 * p + j] = d->ew[j];
-    c.tab = c.alloc_n<double>(tab.size());
-    EG_CUDA(cudaMemcpy(c.tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
-    std::vector<double> mdg(p), mhdg(2 * q);
-    for (int i = 0; i < p; ++i) mdg[i] = d->area * d->mass[i];
-    for (int j = 0; j < q; ++j) {
-      mhdg[j] = d->hy / d->ew[j];
-      mhdg[q + j] = d->hx / d->ew[j];
-    }
-    c.mtab_dg = c.alloc_n<double>(p);
+    const int q = c.q;
+    c.tab = c.alloc_n<double>(eg::tab_size(q));
+    c.mtab_dg = c.alloc_n<double>(c.p);
     c.mtab_hdg = c.alloc_n<double>(2 * q);
-    EG_CUDA(cudaMemcpy(c.mtab_dg, mdg.data(), sizeof(double) * p, cudaMemcpyHostToDevice));
-    EG_CUDA(cudaMemcpy(c.mtab_hdg, mhdg.data(), sizeof(double) * 2 * q, cudaMemcpyHostToDevice));
+    eg::upload_desc(c, *d);
     for (double **v : {&c.u, &c.old, &c.r, &c.du, &c.trial, &c.trial_r, &c.er, &c.tmp_body}) {
       *v = c.alloc_n<double>(c.nu);
-      EG_CUDA(cudaMemset(*v, 0, sizeof(double) * c.nu));
+      EG_CUDA(cudaMemsetAsync(*v, 0, sizeof(double) * c.nu, c.stream));
     }
     for (double **v : {&c.fa, &c.fbb, &c.flw, &c.frw, &c.fpen}) {
       *v = c.alloc_n<double>((size_t)c.nf * q);
-      EG_CUDA(cudaMemset(*v, 0, sizeof(double) * c.nf * q));
+      EG_CUDA(cudaMemsetAsync(*v, 0, sizeof(double) * c.nf * q, c.stream));
     }
     c.D = c.alloc_n<double>(c.nl);
-    EG_CUDA(cudaMemset(c.D, 0, sizeof(double) * c.nl));
+    EG_CUDA(cudaMemsetAsync(c.D, 0, sizeof(double) * c.nl, c.stream));
     c.derr = c.alloc_n<int>(4);
-    EG_CUDA(cudaMemset(c.derr, 0, 4 * sizeof(int)));
+    EG_CUDA(cudaMemsetAsync(c.derr, 0, 4 * sizeof(int), c.stream));
     c.dscal = c.alloc_n<double>(eg::DS_COUNT);
-    EG_CUDA(cudaMemset(c.dscal, 0, eg::DS_COUNT * sizeof(double)));
+    EG_CUDA(cudaMemsetAsync(c.dscal, 0, eg::DS_COUNT * sizeof(double), c.stream));
     c.counter = c.alloc_n<unsigned>(1);
-    EG_CUDA(cudaMemset(c.counter, 0, sizeof(unsigned)));
+    EG_CUDA(cudaMemsetAsync(c.counter, 0, sizeof(unsigned), c.stream));
     c.partials = c.alloc_n<double>((size_t)eg::kRedBlocks * (eg::kMaxRestart + 1));
     c.ctl = c.alloc_n<eg::GmresCtl>(1);
     EG_CUDA(cudaMallocHost(&c.hctl, sizeof(eg::GmresCtl)));
@@ -766,6 +776,18 @@ int eg_recover(eg_ctx *ctx, const double *lam, double *du) {
 int eg_pc_factor(eg_ctx *ctx, int factor) {
   if (!ctx) return EG_ERR_INVALID;
   return guard(ctx, [&] { eg::pc_factor(ctx->c, ctx->c.opts.form, factor != 0); });
+}
+
+int eg_set_desc(eg_ctx *ctx, const eg_desc *d) {
+  if (!ctx || !d) return EG_ERR_INVALID;
+  return guard(ctx, [&] {
+    Ctx &c = ctx->c;
+    if (d->nx != c.desc.nx || d->ny != c.desc.ny || d->k != c.desc.k)
+      eg::fail(EG_ERR_INVALID, "a context keeps its mesh size and degree");
+    for (int i = 0; i < c.p; ++i)
+      if (d->tensor_node[i] != i) eg::fail(EG_ERR_INVALID, "native node order must be lexicographic (x fastest)");
+    eg::upload_desc(c, *d);
+  });
 }
 
 int eg_pc_size(const eg_ctx *ctx, long long *count) {

@@ -290,17 +290,17 @@ struct eg_server {
         std::lock_guard<std::mutex> lk(m);
         req = jobs[id].req;
       }
-      eg_request_result res{};
-      int rc = EG_OK;
-      if (!ctx) {
-        eg_desc d{};
-        rc = eg_desc_simple_wave(&d, req.nx, req.ny, req.k, req.alpha_deg, 3.0, 1.1);
+      eg_desc d{};
+      int rc = eg_desc_simple_wave(&d, req.nx, req.ny, req.k, req.alpha_deg, 3.0, 1.1);
+      if (rc == EG_OK && ctx) {
+        rc = eg_set_desc(ctx, &d);  // a pooled context of this size: this request's geometry
+      } else if (rc == EG_OK) {
         eg_opts eo{};
         eg_opts_default(&eo);
         eo.form = req.form;
         eo.precond = req.precond;
         eo.precision = req.precision;
-        if (rc == EG_OK) rc = eg_create(&d, &eo, &ctx);
+        rc = eg_create(&d, &eo, &ctx);
       }
       eg_run_result rr{};
       std::vector<double> state;

@@ -291,10 +291,9 @@ static Frozen frozen_of(Ctx &c) { return Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpe
 void launch_freeze(Ctx &c, const double *u, bool check_admissible) {
   if (check_admissible) {
     launch_admissible(c, u);
+    EG_CUDA(cudaMemcpyAsync(c.herr + 1, c.derr + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
-    int ok = 1;
-    EG_CUDA(cudaMemcpy(&ok, c.derr + 1, sizeof(int), cudaMemcpyDeviceToHost));
-    if (!ok) fail(EG_ERR_INADMISSIBLE, "Old state is inadmissible; refine mesh");
+    if (!c.herr[1]) fail(EG_ERR_INADMISSIBLE, "Old state is inadmissible; refine mesh");
   }
   EG_CUDA(cudaMemsetAsync(c.dscal + DS_WAVE, 0, sizeof(double), c.stream));
   const int total = c.nf * c.q;

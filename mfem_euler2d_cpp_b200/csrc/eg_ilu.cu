@@ -683,7 +683,8 @@ void build_plan(Ctx &c, int form) {
   // schedules (the forward one is also the factor's)
   auto upload = [&](const std::vector<int> &v) {
     int *d = c.alloc_n<int>(v.size());
-    EG_CUDA(cudaMemcpy(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice));
+    EG_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, c.stream));
+    c.sync();  // the host vector is local
     return d;
   };
   for (int back = 0; back < 2; ++back) {
@@ -739,9 +740,9 @@ void build_plan(Ctx &c, int form) {
   if (hdg) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
   if (!P.staged) P.work = c.alloc_n<double>((size_t)G * 3 * BB);
   P.progress = c.alloc_n<unsigned long long>(G);
-  EG_CUDA(cudaMemset(P.progress, 0, sizeof(unsigned long long) * G));
+  EG_CUDA(cudaMemsetAsync(P.progress, 0, sizeof(unsigned long long) * G, c.stream));
   P.abort = c.alloc_n<int>(1);
-  EG_CUDA(cudaMemset(P.abort, 0, sizeof(int)));
+  EG_CUDA(cudaMemsetAsync(P.abort, 0, sizeof(int), c.stream));
   P.epoch = 0;
   P.built = true;
 }

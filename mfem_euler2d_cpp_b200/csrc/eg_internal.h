@@ -228,6 +228,9 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er);
 void launch_schur_jacobi(Ctx &c, bool factor);
 // x = Inv b for explicit block inverses (Schur block Jacobi apply).
 void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x);
+// ---- eg_api.cu ----
+// Sets the context's description (geometry, tables, metrics) for its size.
+void upload_desc(Ctx &c, const eg_desc &d);
 // ---- block ILU(0) (eg_ilu.cu) ----
 // Fill (and with factor set, factor) the ILU of `form` at the current state /
 // condensation; x = ILU^{-1} b.

@@ -162,6 +162,10 @@ __global__ void __launch_bounds__(kRedThreads)
 constexpr int kCgsBlocks = 592;  // 4 CTAs per SM
 constexpr int kCgsThreads = 256;
 static_assert(kCgsBlocks * 24 <= kRedBlocks * (kMaxRestart + 1), "partials hold every CTA's column sums");
+// Grid of the register CGS passes for a vector of length N: about four
+// elements per thread, at most kCgsBlocks CTAs (a function of N only, so the
+// summation order stays fixed for a given problem).
+inline int cgs_grid(int N) { return std::max(1, std::min(kCgsBlocks, (N + 4 * kCgsThreads - 1) / (4 * kCgsThreads))); }
 
 template <int NC>
 __device__ __forceinline__ void cta_reduce_columns(double (&acc)[NC], int nc, double *red /* [8][NC] */,
@@ -359,8 +363,9 @@ static int vec_grid(int N) { return std::max(1, std::min((N + 255) / 256, 148 * 
 template <class T>
 void launch_wnorm2_t(Ctx &c, const T *x, int N, const double *mtab, int period, int slot) {
   ProfScope ps(c, EG_K_KRYLOV, 1);
-  wnorm2_kernel<T><<<kRedBlocks, kRedThreads, 0, c.stream>>>(N, x, mtab, period, c.partials, c.counter,
-                                                             c.dscal + slot);
+  // a grid that depends on N only keeps the summation order fixed per problem
+  const int grid = std::max(1, std::min(kRedBlocks, (N + 4 * kRedThreads - 1) / (4 * kRedThreads)));
+  wnorm2_kernel<T><<<grid, kRedThreads, 0, c.stream>>>(N, x, mtab, period, c.partials, c.counter, c.dscal + slot);
   EG_CUDA(cudaGetLastError());
 }
 void launch_wnorm2(Ctx &c, const double *x, int N, const double *mtab, int period, int slot) {
@@ -401,11 +406,12 @@ void launch_fill(Ctx &c, int N, double v, double *out) {
 // The three CGS2 passes of Arnoldi step j (src/linear.cpp:104-118).
 template <class T, int NC>
 void cgs_reg_passes(Ctx &c, int N, T *w, const T *V, size_t ldv, int nc, const double *mtab, int period, int R) {
-  cgs_reg_kernel<0, T, NC><<<kCgsBlocks, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+  const int grid = cgs_grid(N);
+  cgs_reg_kernel<0, T, NC><<<grid, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
                                                                      c.counter, c.ctl, R);
-  cgs_reg_kernel<1, T, NC><<<kCgsBlocks, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+  cgs_reg_kernel<1, T, NC><<<grid, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
                                                                      c.counter, c.ctl, R);
-  cgs_reg_kernel<2, T, NC><<<kCgsBlocks, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+  cgs_reg_kernel<2, T, NC><<<grid, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
                                                                      c.counter, c.ctl, R);
 }
 template <class T>

@@ -329,7 +329,8 @@ int eg_run(eg_ctx *ctx, const eg_run_opts *ro, eg_run_result *res) {
     out.final_time = s.time;
     out.time_steps = s.step;
     std::vector<double> u(c.nu);
-    EG_CUDA(cudaMemcpy(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost));
+    EG_CUDA(cudaMemcpyAsync(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
     eg::host::errors(c.desc, u.data(), s.time, out.errors);
     double fin[4];
     eg::host::integral(c.desc, u.data(), fin);

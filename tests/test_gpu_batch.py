@@ -64,6 +64,18 @@ def test_server_result_same_alone_and_in_the_mix():
             assert r.status == capi.OK and r.finish_s >= r.start_s >= r.submit_s
 
 
+def test_pooled_context_takes_the_new_request_geometry():
+    """A finished context is reused for a request of the same size but another
+    angle: the result must be the one a fresh context gives."""
+    nu = 16 * 16 * 4 * 9
+    with capi.Server(workers=1, keep_states=True) as s:
+        first = s.submit(16, 16, 2, 25.0, steps=1, newton_steps=2)
+        second = s.submit(16, 16, 2, 65.0, steps=1, newton_steps=2)
+        s.drain()
+        assert s.poll(first).status == capi.OK and s.poll(second).status == capi.OK
+        np.testing.assert_array_equal(s.state(second, nu), _alone(16, 16, 2, 65.0))
+
+
 def test_server_admission_respects_the_memory_budget():
     with capi.Server(workers=1, keep_contexts=False) as s:
         rid = s.submit(24, 24, 3, 40.0, steps=1, newton_steps=1)
