@@ -702,6 +702,7 @@ struct GjgCfg {
   static constexpr int NB = 16;                      // panel width
   static constexpr int NPAN = (M + NB - 1) / NB;
   static constexpr int MT = (M + 7) / 8;            // 8-row tiles
+  static constexpr int RU = 6;                       // row tiles per load round of the update
   static constexpr size_t SMEM = sizeof(double) * ((size_t)2 * NB * M + (size_t)NB * NC + 2 * NB * NB) +
                                  sizeof(int) * (size_t)(3 * M + NB);
 };
@@ -869,22 +870,36 @@ __global__ void __launch_bounds__(256, 1)
           bf[ks] = cc < ntr ? top[(size_t)(4 * ks + tq) * NC + cc] : 0.;
         }
         const int col0 = cs + ct * 8 + 2 * tq;
-        for (int rt = 0; rt < C::MT; ++rt) {
-          const int ra = rt * 8 + gq;  // row of this lane's A fragment and C values
-          double c0v = 0., c1v = 0.;
-          const bool rok = ra < M;
-          if (rok && col0 < NC) c0v = W[(size_t)col0 * M + ra];
-          if (rok && col0 + 1 < NC) c1v = W[(size_t)(col0 + 1) * M + ra];
-          const int pi = rok ? pidx[ra] : -1;
+        const bool ok0 = col0 < NC, ok1 = col0 + 1 < NC;
+        // GjgCfg::RU row tiles per round: their loads are all in flight before the MMAs
+        for (int rt0 = 0; rt0 < C::MT; rt0 += C::RU) {
+          double cv[C::RU][2];
 #pragma unroll
-          for (int ks = 0; ks < NB / 4; ++ks) {
-            const int k = 4 * ks + tq;
-            double a = rok ? P0[(size_t)k * M + ra] : 0.;
-            if (pi == k) a -= 1.;
-            dmma_m8n8k4(c0v, c1v, -a, bf[ks]);
+          for (int u = 0; u < C::RU; ++u) {
+            const int ra = (rt0 + u) * 8 + gq;  // row of this lane's A fragment and C values
+            const bool rok = ra < M;
+            cv[u][0] = rok && ok0 ? W[(size_t)col0 * M + ra] : 0.;
+            cv[u][1] = rok && ok1 ? W[(size_t)(col0 + 1) * M + ra] : 0.;
           }
-          if (rok && col0 < NC) W[(size_t)col0 * M + ra] = c0v;
-          if (rok && col0 + 1 < NC) W[(size_t)(col0 + 1) * M + ra] = c1v;
+#pragma unroll
+          for (int u = 0; u < C::RU; ++u) {
+            const int ra = (rt0 + u) * 8 + gq;
+            const bool rok = ra < M;
+            const int pi = rok ? pidx[ra] : -1;
+#pragma unroll
+            for (int ks = 0; ks < NB / 4; ++ks) {
+              const int k = 4 * ks + tq;
+              double a = rok ? P0[(size_t)k * M + ra] : 0.;
+              if (pi == k) a -= 1.;
+              dmma_m8n8k4(cv[u][0], cv[u][1], -a, bf[ks]);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < C::RU; ++u) {
+            const int ra = (rt0 + u) * 8 + gq;
+            if (ra < M && ok0) W[(size_t)col0 * M + ra] = cv[u][0];
+            if (ra < M && ok1) W[(size_t)(col0 + 1) * M + ra] = cv[u][1];
+          }
         }
       }
       __syncthreads();  // every warp has finished reading pidx for this panel
