@@ -731,10 +731,14 @@ struct GjgCfg {
   static constexpr int RU = 6;                       // row tiles per load round of the update
   static constexpr size_t SMEM = sizeof(double) * ((size_t)2 * NB * M + (size_t)NB * NC + 2 * NB * NB) +
                                  sizeof(int) * (size_t)(3 * M + NB);
+  // two CTAs per SM where their shared memory fits (k = 5, 6): one CTA's
+  // serial pivot chain then overlaps the other's trailing update
+  static constexpr int MINB =
+      2 * (SMEM + sizeof(CondenseShared<Q>) + 2048) <= 227 * 1024 ? 2 : 1;
 };
 
 template <int Q>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, GjgCfg<Q>::MINB)
     condense_gjg_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
                         const double *__restrict__ r, double *XY, double *Cb, double *sf, double *contrib,
                         double *panels, double *work, int *err) {
@@ -1138,7 +1142,9 @@ static void launch_condense_gjg(Ctx &c, const double *u, const double *r) {
   using C = GjgCfg<Q>;
   auto kern = condense_gjg_kernel<Q>;
   EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-  const int grid = std::min(c.n, sm_count_hdg());
+  int per_sm = 0;
+  EG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, C::SMEM));
+  const int grid = std::min(c.n, std::max(1, std::min(per_sm, C::MINB)) * sm_count_hdg());
   if (c.work_gj == nullptr || c.work_gj_slots < grid) {
     c.work_gj = c.alloc_n<double>((size_t)grid * C::M * C::NC);
     c.work_gj_slots = grid;
