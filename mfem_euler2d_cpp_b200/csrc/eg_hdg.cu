@@ -781,32 +781,33 @@ __global__ void __launch_bounds__(256, GjgCfg<Q>::MINB)
       __syncthreads();
       for (int j = 0; j < nb; ++j) {
         if (warp == 0) {
-          double best = -1.;
+          // largest |Pw[j][r]| among unused rows, first row on ties, NaN never
+          // chosen: magnitudes compared as IEEE bit patterns (integer compares,
+          // three warp reductions)
+          constexpr unsigned long long kAbs = 0x7fffffffffffffffull, kInf = 0x7ff0000000000000ull;
+          unsigned long long best = 0ull;
           int bi = M;
           for (int rr = lane; rr < M; rr += 32) {
             if (used[rr]) continue;
-            const double v = fabs(Pw[(size_t)j * M + rr]);
-            if (v > best) {
-              best = v;
+            const unsigned long long bits =
+                (unsigned long long)__double_as_longlong(Pw[(size_t)j * M + rr]) & kAbs;
+            if (bits <= kInf && (bi == M || bits > best)) {
+              best = bits;
               bi = rr;
             }
           }
-#pragma unroll
-          for (int off = 16; off > 0; off >>= 1) {
-            const double ob = __shfl_down_sync(0xffffffffu, best, off);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-            if (ob > best || (ob == best && oi < bi)) {
-              best = ob;
-              bi = oi;
-            }
-          }
+          const unsigned hi = (unsigned)(best >> 32), lo = (unsigned)best;
+          const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+          const bool c1 = bi < M && hi == mhi;
+          const unsigned mlo = __reduce_max_sync(0xffffffffu, c1 ? lo : 0u);
+          bi = (int)__reduce_min_sync(0xffffffffu, c1 && lo == mlo ? (unsigned)bi : (unsigned)M);
           if (lane == 0) {
             const double pv = bi < M ? Pw[(size_t)j * M + bi] : 0.;  // an all-NaN column is singular
             if (!(fabs(pv) > 0.)) {
               sing = 1;
               bi = 0;
             }
-            pivval = pv;
+            pivval = pivot_reciprocal(pv);
             prow[j] = bi;
             piv[c0 + j] = bi;
             used[bi] = 1;
@@ -816,7 +817,7 @@ __global__ void __launch_bounds__(256, GjgCfg<Q>::MINB)
         __syncthreads();
         if (sing) break;
         const int pr = prow[j];
-        const double inv = 1.0 / pivval;
+        const double inv = pivval;  // 1 / pivot
         const int rest = nb - j - 1;
         for (int o = threadIdx.x; o < rest * M; o += blockDim.x) {
           const int jj = j + 1 + o / M, rr = o % M;
@@ -837,16 +838,18 @@ __global__ void __launch_bounds__(256, GjgCfg<Q>::MINB)
       __syncthreads();
       if (warp == 0) {
         for (int j = 0; j < NB; ++j) {
-          // pivot among rows j..NB-1 of column j
-          double best = -1.;
-          int bi = j;
-          for (int i = j; i < NB; ++i) {
-            const double v = fabs(Tm[i * 2 * NB + j]);
-            if (v > best) {
-              best = v;
-              bi = i;
-            }
-          }
+          // pivot among rows j..NB-1 of column j (lane i holds row i): largest
+          // magnitude, first row on ties, NaN never chosen (row j if all are)
+          constexpr unsigned long long kAbs = 0x7fffffffffffffffull, kInf = 0x7ff0000000000000ull;
+          const unsigned long long bits =
+              lane < NB ? (unsigned long long)__double_as_longlong(Tm[lane * 2 * NB + j]) & kAbs : 0ull;
+          const bool cand = lane >= j && lane < NB && bits <= kInf;
+          const unsigned hi = cand ? (unsigned)(bits >> 32) : 0u, lo = cand ? (unsigned)bits : 0u;
+          const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+          const bool c1 = cand && hi == mhi;
+          const unsigned mlo = __reduce_max_sync(0xffffffffu, c1 ? lo : 0u);
+          const unsigned first = __reduce_min_sync(0xffffffffu, c1 && lo == mlo ? (unsigned)lane : 32u);
+          const int bi = first < 32u ? (int)first : j;
           const double pv = Tm[bi * 2 * NB + j];
           __syncwarp();
           if (bi != j) {  // swap rows j and bi (lane = column)
