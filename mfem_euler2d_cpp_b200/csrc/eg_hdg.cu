@@ -1088,6 +1088,101 @@ __global__ void __launch_bounds__(64)
   }
 }
 
+// The same blocks inverted by one warp per face for T <= 32: lane r holds row
+// r of [S | I] in registers and Gauss-Jordan runs with partial pivoting over
+// the rows not yet used as pivot rows (largest magnitude, first row on ties,
+// NaN never chosen; a zero pivot is singular, as in LU with row exchanges).
+// Rows never move: the pivot row of step k ends up holding row k of S^{-1}.
+// The pivot search is three warp reductions on IEEE bit patterns and the
+// normalised pivot row is broadcast by shuffles, so no step needs a barrier.
+// `pivots` receives the pivot row of every step.
+template <int T>
+__global__ void __launch_bounds__(128)
+    schur_jacobi_warp_kernel(int nx, int ny, int nf, const double *__restrict__ D,
+                             const double *__restrict__ panels, double *blocks, int *pivots, bool factor,
+                             int *err) {
+  static_assert(T <= 32, "one row per lane");
+  constexpr unsigned long long kAbs = 0x7fffffffffffffffull, kInf = 0x7ff0000000000000ull;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int f = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); f < nf; f += nwarps) {
+    const int L = f >> 1, ls = (f & 1) ? 3 : 1;
+    const int R = neighbour(L, ls, nx, ny), rs = ls - 1;
+    const double *pl = panels + ((size_t)L * 4 + ls) * T * T;
+    const double *pr = panels + ((size_t)R * 4 + rs) * T * T;
+    const bool row_ok = lane < T;
+    const double d = row_ok ? D[(size_t)f * T + lane] : 0.;
+    double sr[T], xr[T];
+#pragma unroll
+    for (int c = 0; c < T; ++c) {
+      sr[c] = row_ok ? ((lane == c ? d : 0.) - pl[c * T + lane]) - pr[c * T + lane] : 0.;
+      xr[c] = lane == c ? 1. : 0.;
+    }
+    double *out = blocks + (size_t)f * T * T;
+    if (!factor) {
+      if (row_ok) {
+#pragma unroll
+        for (int c = 0; c < T; ++c) out[c * T + lane] = sr[c];
+        pivots[(size_t)f * T + lane] = lane;
+      }
+      continue;
+    }
+    bool un = row_ok;
+    int pos = 0;
+    bool singular = false;
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+      double sk = 0.;
+#pragma unroll
+      for (int c = 0; c < T; ++c)
+        if (c == k) sk = sr[c];
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(sk) & kAbs;
+      const bool cand = un && bits <= kInf;
+      const unsigned hi = cand ? (unsigned)(bits >> 32) : 0u, lo = cand ? (unsigned)bits : 0u;
+      const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+      const bool c1 = cand && hi == mhi;
+      const unsigned mlo = __reduce_max_sync(0xffffffffu, c1 ? lo : 0u);
+      const unsigned pw = __reduce_min_sync(0xffffffffu, c1 && lo == mlo ? (unsigned)lane : 32u);
+      // a zero pivot (warp-uniform) marks the block singular; the remaining
+      // steps run on row 0 and their results are discarded
+      const bool zero = pw >= 32u || (mhi == 0u && mlo == 0u);
+      singular = singular || zero;
+      const int p = zero ? 0 : (int)pw;
+      const double l = sk;
+      const double ip = 1.0 / __shfl_sync(0xffffffffu, l, p);
+      const bool me = lane == p;
+#pragma unroll
+      for (int c = 0; c < T; ++c) {
+        if (c > k) {
+          const double v = __shfl_sync(0xffffffffu, sr[c], p) * ip;
+          sr[c] = me ? v : sr[c] - l * v;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < T; ++c) {
+        const double v = __shfl_sync(0xffffffffu, xr[c], p) * ip;
+        xr[c] = me ? v : xr[c] - l * v;
+      }
+#pragma unroll
+      for (int c = 0; c < T; ++c)
+        if (c == k) sr[c] = me ? 1. : 0.;
+      if (me) {
+        un = false;
+        pos = k;
+      }
+    }
+    if (singular) {
+      if (lane == 0) raise_err(err, DERR_SINGULAR_JACOBI);
+      continue;
+    }
+    if (row_ok) {
+#pragma unroll
+      for (int c = 0; c < T; ++c) out[c * T + pos] = xr[c];
+      pivots[(size_t)f * T + pos] = lane;
+    }
+  }
+}
+
 // x_b = Inv_b b_b for column-major bs x bs inverses; one thread per output row.
 __global__ void __launch_bounds__(256) block_gemv_kernel(const double *__restrict__ inv, int nblocks, int bs,
                                                          const double *__restrict__ b,
@@ -1234,14 +1329,19 @@ void launch_schur_jacobi(Ctx &c, bool factor) {
   c.ensure_pc_hdg();
   ProfScope ps(c, EG_K_SCHUR_JACOBI, 1);
   const int grid = std::min(c.nf, sm_count_hdg() * 32);
+  const int wgrid = std::min((c.nf + 3) / 4, sm_count_hdg() * 32);  // 4 warps (faces) per CTA
   switch (c.t) {
-#define EG_SJ(TT)                                                                                 \
-  case TT:                                                                                        \
-    schur_jacobi_kernel<TT><<<grid, 64, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.D, c.panels, \
-                                                       c.pc_hdg, c.piv_hdg, factor, c.derr);             \
+#define EG_SJW(TT)                                                                                     \
+  case TT:                                                                                             \
+    schur_jacobi_warp_kernel<TT><<<wgrid, 128, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.D, c.panels, \
+                                                              c.pc_hdg, c.piv_hdg, factor, c.derr);      \
     break;
-    EG_SJ(4) EG_SJ(8) EG_SJ(12) EG_SJ(16) EG_SJ(20) EG_SJ(24) EG_SJ(28) EG_SJ(32) EG_SJ(36)
-#undef EG_SJ
+    EG_SJW(4) EG_SJW(8) EG_SJW(12) EG_SJW(16) EG_SJW(20) EG_SJW(24) EG_SJW(28) EG_SJW(32)
+#undef EG_SJW
+    case 36:
+      schur_jacobi_kernel<36><<<grid, 64, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.D, c.panels, c.pc_hdg,
+                                                         c.piv_hdg, factor, c.derr);
+      break;
     default:
       fail(EG_ERR_INVALID, "unsupported trace block size");
   }

@@ -70,6 +70,47 @@ __global__ void __launch_bounds__(kRedThreads)
   }
 }
 
+// Givens update of Hessenberg column j and the convergence test
+// (src/linear.cpp:123-136), run by the last CTA of the norm pass once
+// h(j+1, j) = next is known: the column and the earlier rotations are staged
+// in shared memory by the CTA, thread 0 applies the chain.
+__device__ void givens_step(GmresCtl *ctl, int R, int j, double *st /* 3 * (kMaxRestart + 1) */) {
+  const int ld = R + 1;
+  double *hc = st, *cs = st + (kMaxRestart + 1), *sn = cs + (kMaxRestart + 1);
+  for (int i = threadIdx.x; i <= j + 1; i += blockDim.x) hc[i] = ctl->h[i + ld * j];
+  for (int i = threadIdx.x; i < j; i += blockDim.x) {
+    cs[i] = ctl->cs[i];
+    sn[i] = ctl->sn[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < j; ++i) {
+      const double u = hc[i], v = hc[i + 1];
+      hc[i] = cs[i] * u + sn[i] * v;
+      hc[i + 1] = -sn[i] * u + cs[i] * v;
+    }
+    const double d = hypot(hc[j], hc[j + 1]);
+    if (!(isfinite(d) && d > 0)) {
+      ctl->err = 1;
+      ctl->stop = 1;
+    } else {
+      const double c = hc[j] / d, s = hc[j + 1] / d;
+      hc[j] = d;
+      hc[j + 1] = 0.;
+      const double gj = ctl->g[j];
+      ctl->cs[j] = c;
+      ctl->sn[j] = s;
+      ctl->g[j + 1] = -s * gj;
+      ctl->g[j] = c * gj;
+      ctl->count = j + 1;
+      ctl->stop = (fabs(ctl->g[j + 1]) <= ctl->abs_tol || ctl->next <= DBL_MIN) ? 1 : 0;
+      ctl->j = j + 1;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= j + 1; i += blockDim.x) ctl->h[i + ld * j] = hc[i];
+}
+
 // ------------------------------------------------------------ CGS2 passes
 // MODE 0: proj = V^T (metric w)                        (first pass)
 // MODE 1: w -= V proj_in; proj = V^T (metric w)        (second pass)
@@ -112,6 +153,8 @@ __global__ void __launch_bounds__(kRedThreads)
         ctl->h[(j + 1) + (R + 1) * j] = next;
         *counter = 0;
       }
+      __syncthreads();
+      givens_step(ctl, R, j, red);
     }
     return;
   }
@@ -194,7 +237,7 @@ __global__ void __launch_bounds__(kCgsThreads)
   __shared__ double red[8 * NC];
   __shared__ double mt[2 * EG_MAX_P];
   __shared__ double pin[NC];
-  __shared__ double fin[kCgsThreads];
+  __shared__ double gst[MODE == 2 ? 3 * (kMaxRestart + 1) : 1];  // Givens staging (norm pass)
   for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
   if (MODE > 0)
     for (int i = threadIdx.x; i < ncols; i += blockDim.x) pin[i] = ctl->proj[i];
@@ -229,28 +272,29 @@ __global__ void __launch_bounds__(kCgsThreads)
   const int nred = MODE == 2 ? 1 : ncols;
   cta_reduce_columns<NC>(acc, nred, red, partials, gridDim.x);
   if (last_block(counter)) {
-    for (int c = 0; c < nred; ++c) {
+    // one warp per column: each lane adds a fixed stride of the CTA partials
+    // in order, then a warp tree (fixed order: bitwise reproducible)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < nred; c += kCgsThreads / 32) {
       double t = 0.;
-      for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) t += partials[(size_t)c * gridDim.x + b];
-      fin[threadIdx.x] = t;
-      __syncthreads();
-      for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) fin[threadIdx.x] += fin[threadIdx.x + s];
-        __syncthreads();
-      }
-      if (threadIdx.x == 0) {
-        const double tot = fin[0];
+      for (int b = lane; b < (int)gridDim.x; b += 32) t += partials[(size_t)c * gridDim.x + b];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+      if (lane == 0) {
         if (MODE == 2) {
-          const double next = sqrt(tot);
+          const double next = sqrt(t);
           ctl->next = next;
           ctl->inv_next = next > 0 ? 1. / next : 0.;
           ctl->h[(j + 1) + (R + 1) * j] = next;
         } else {
-          ctl->proj[c] = tot;
-          ctl->h[c + (R + 1) * j] += tot;
+          ctl->proj[c] = t;
+          ctl->h[c + (R + 1) * j] += t;
         }
       }
-      __syncthreads();
+    }
+    if (MODE == 2) {
+      __syncthreads();  // next and h(j+1, j) written by thread 0
+      givens_step(ctl, R, j, gst);
     }
     if (threadIdx.x == 0) *counter = 0;
   }
@@ -264,34 +308,6 @@ __global__ void normalize_kernel(int N, const T *__restrict__ w, T *__restrict__
   const double s = 1. / next;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     vnext[i] = (T)((double)w[i] * s);
-}
-
-// Givens update of Hessenberg column j and the convergence test
-// (src/linear.cpp:123-136). Single thread.
-__global__ void givens_kernel(GmresCtl *ctl, int R) {
-  const int j = ctl->j;
-  double *h = ctl->h;
-  const int ld = R + 1;
-  for (int i = 0; i < j; ++i) {
-    const double u = h[i + ld * j], v = h[(i + 1) + ld * j];
-    h[i + ld * j] = ctl->cs[i] * u + ctl->sn[i] * v;
-    h[(i + 1) + ld * j] = -ctl->sn[i] * u + ctl->cs[i] * v;
-  }
-  const double d = hypot(h[j + ld * j], h[(j + 1) + ld * j]);
-  if (!(isfinite(d) && d > 0)) {
-    ctl->err = 1;
-    ctl->stop = 1;
-    return;
-  }
-  ctl->cs[j] = h[j + ld * j] / d;
-  ctl->sn[j] = h[(j + 1) + ld * j] / d;
-  h[j + ld * j] = d;
-  h[(j + 1) + ld * j] = 0.;
-  ctl->g[j + 1] = -ctl->sn[j] * ctl->g[j];
-  ctl->g[j] *= ctl->cs[j];
-  ctl->count = j + 1;
-  ctl->stop = (fabs(ctl->g[j + 1]) <= ctl->abs_tol || ctl->next <= DBL_MIN) ? 1 : 0;
-  ctl->j = j + 1;
 }
 
 // Upper-triangular solve for the Krylov coefficients (src/linear.cpp:138-142).
@@ -479,10 +495,9 @@ double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs
       ops.apply(c, z, w);
       const int nc = j + 1;
       {
-        ProfScope ps(c, EG_K_KRYLOV, 5);
+        ProfScope ps(c, EG_K_KRYLOV, 4);
         cgs_passes<T>(c, N, w, V, ldv, nc, ops.mtab, ops.period, R);
         normalize_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, w, V + (size_t)(j + 1) * ldv, c.ctl);
-        givens_kernel<<<1, 1, 0, c.stream>>>(c.ctl, R);
         EG_CUDA(cudaGetLastError());
       }
       EG_CUDA(cudaMemcpyAsync(&c.hctl->stop, &c.ctl->stop, 2 * sizeof(int), cudaMemcpyDeviceToHost,
