@@ -181,6 +181,8 @@ struct HdgOps : LinearOps {
     N = c.nl;
     mtab = c.mtab_hdg;
     period = 2 * c.t;
+    // the block-Jacobi and Schur kernels honour Ctx::skip; the ILU sweeps do not
+    group = c.opts.precond == EG_PC_BLOCK_ILU0 ? 1 : kArnoldiGroup;
   }
   void apply(Ctx &c, const double *x, double *y) override { launch_schur_apply(c, x, y); }
   void precondition(Ctx &c, const double *b, double *x) override {

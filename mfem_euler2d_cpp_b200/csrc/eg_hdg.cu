@@ -962,8 +962,9 @@ template <int Q, bool RECOVER>
 __global__ void __launch_bounds__(128)
     cell_gemv_kernel(Geo g, const double *__restrict__ tab, const double *__restrict__ XY,
                      const double *__restrict__ Cb, const double *__restrict__ v,
-                     double *__restrict__ out) {
+                     double *__restrict__ out, const int *__restrict__ skip) {
   constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
+  if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
   __shared__ STab<Q> st;
   __shared__ double vl[4 * T], mid[M];
   load_tables<Q>(st, tab);
@@ -1009,7 +1010,8 @@ __global__ void __launch_bounds__(128)
 // y_f = D_f v_f - contrib[L][ls] - contrib[R][rs]  (one thread per trace dof)
 __global__ void face_combine_kernel(int nx, int ny, int T, int nl, const double *__restrict__ D,
                                     const double *__restrict__ v, const double *__restrict__ contrib,
-                                    double sign_v, double *__restrict__ y) {
+                                    double sign_v, double *__restrict__ y, const int *__restrict__ skip) {
+  if (skip != nullptr && *skip) return;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nl) return;
   const int f = idx / T, i = idx % T;
@@ -1186,7 +1188,8 @@ __global__ void __launch_bounds__(128)
 // x_b = Inv_b b_b for column-major bs x bs inverses; one thread per output row.
 __global__ void __launch_bounds__(256) block_gemv_kernel(const double *__restrict__ inv, int nblocks, int bs,
                                                          const double *__restrict__ b,
-                                                         double *__restrict__ x) {
+                                                         double *__restrict__ x, const int *__restrict__ skip) {
+  if (skip != nullptr && *skip) return;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long long)nblocks * bs) return;
   const int blk = (int)(id / bs), row = (int)(id % bs);
@@ -1285,7 +1288,7 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
   // rhs_f = contrib_L + contrib_R (s.rhs = 0; rhs[ids] += C y)
   const int blocks = (c.nl + 255) / 256;
   face_combine_kernel<<<blocks, 256, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.t, c.nl, nullptr, c.rhs,
-                                                    c.contrib, -1.0, c.rhs);
+                                                    c.contrib, -1.0, c.rhs, nullptr);
   EG_CUDA(cudaGetLastError());
   c.condensed = true;
 }
@@ -1294,11 +1297,11 @@ void launch_schur_apply(Ctx &c, const double *v, double *y) {
   ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
   const int grid = std::min(c.n, sm_count_hdg() * 16);
   EG_DISPATCH_Q(c.q, (cell_gemv_kernel<Q, false><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb,
-                                                                            v, c.contrib)));
+                                                                            v, c.contrib, c.skip)));
   EG_CUDA(cudaGetLastError());
   const int blocks = (c.nl + 255) / 256;
   face_combine_kernel<<<blocks, 256, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.t, c.nl, c.D, v,
-                                                    c.contrib, 1.0, y);
+                                                    c.contrib, 1.0, y, c.skip);
   EG_CUDA(cudaGetLastError());
 }
 
@@ -1306,7 +1309,7 @@ void launch_recover(Ctx &c, const double *lam, double *du) {
   ProfScope ps(c, EG_K_RECOVER, 1);
   const int grid = std::min(c.n, sm_count_hdg() * 16);
   EG_DISPATCH_Q(c.q, (cell_gemv_kernel<Q, true><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb,
-                                                                           lam, du)));
+                                                                           lam, du, nullptr)));
   EG_CUDA(cudaGetLastError());
 }
 
@@ -1321,7 +1324,7 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er) {
 void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x) {
   ProfScope ps(c, EG_K_PC_APPLY, 1);
   const long long total = (long long)nblocks * bs;
-  block_gemv_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(inv, nblocks, bs, b, x);
+  block_gemv_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(inv, nblocks, bs, b, x, c.skip);
   EG_CUDA(cudaGetLastError());
 }
 

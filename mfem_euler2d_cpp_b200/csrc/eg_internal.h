@@ -93,11 +93,18 @@ struct LinearOpsT {
   int N;
   const double *mtab;  // metric table (device)
   int period;          // metric period in entries
+  // Arnoldi steps GMRES enqueues per host check of the stop flag; above 1
+  // only for operators whose kernels return at once while Ctx::skip is set
+  int group = 1;
   virtual void apply(Ctx &c, const T *x, T *y) = 0;
   virtual void precondition(Ctx &c, const T *b, T *x) = 0;
   virtual ~LinearOpsT() = default;
 };
 using LinearOps = LinearOpsT<double>;
+// Arnoldi steps per host check of the GMRES stop flag for operators whose
+// kernels honour Ctx::skip: a group costs at most kArnoldiGroup - 1 steps of
+// no-op launches after convergence and saves a host round trip per step.
+constexpr int kArnoldiGroup = 4;
 
 // Krylov workspace of one vector type: basis (R+1 columns, leading dimension
 // ld) and the work vectors of the solver.
@@ -173,6 +180,9 @@ struct Ctx {
          *kx = nullptr;
   GmresCtl *ctl = nullptr;
   GmresCtl *hctl = nullptr;  // pinned mirror
+  // set while GMRES enqueues a group of Arnoldi steps: the operator kernels
+  // of those steps return at once when *skip (the device stop flag) is set
+  const int *skip = nullptr;
   double *partials = nullptr;  // kRedBlocks * (kMaxRestart+1)
   unsigned *counter = nullptr;
   // error word (derr[0]) and admissibility flag (derr[1])

@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(kRedThreads)
   __shared__ double red[kRedThreads];
   __shared__ double mt[2 * EG_MAX_P];
   __shared__ double pin[kMaxRestart + 1];
+  if (ctl->stop) return;  // speculative Arnoldi step after convergence
   for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
   if (MODE > 0)
     for (int i = threadIdx.x; i < ncols; i += blockDim.x) pin[i] = ctl->proj[i];
@@ -238,6 +239,7 @@ __global__ void __launch_bounds__(kCgsThreads)
   __shared__ double mt[2 * EG_MAX_P];
   __shared__ double pin[NC];
   __shared__ double gst[MODE == 2 ? 3 * (kMaxRestart + 1) : 1];  // Givens staging (norm pass)
+  if (ctl->stop) return;  // speculative Arnoldi step after convergence
   for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
   if (MODE > 0)
     for (int i = threadIdx.x; i < ncols; i += blockDim.x) pin[i] = ctl->proj[i];
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(kCgsThreads)
 template <class T>
 __global__ void normalize_kernel(int N, const T *__restrict__ w, T *__restrict__ vnext, const GmresCtl *ctl) {
   const double next = ctl->next;
-  if (!(next > 0)) return;
+  if (!(next > 0) || ctl->stop) return;  // a stopped cycle never reads V_{j+1}
   const double s = 1. / next;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     vnext[i] = (T)((double)w[i] * s);
@@ -489,23 +491,37 @@ double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs
       cycle_init_kernel<<<1, 256, 0, c.stream>>>(c.ctl, R, beta, tol * rhs_norm);
       EG_CUDA(cudaGetLastError());
     }
-    for (int j = 0; j < R && iterations < limit; ++j) {
-      const T *vj = V + (size_t)j * ldv;
-      ops.precondition(c, vj, z);
-      ops.apply(c, z, w);
-      const int nc = j + 1;
-      {
+    // Arnoldi steps are enqueued in groups of ops.group with one host check
+    // of the device stop flag per group; the steps of a group that follow the
+    // converged one return at once (Ctx::skip, and the stop check of the CGS
+    // and normalisation kernels), so iterates and counts are those of a
+    // check after every step.
+    for (int j = 0; j < R && iterations < limit;) {
+      const int group = std::max(1, std::min(ops.group, std::min(R - j, limit - iterations)));
+      struct SkipGuard {
+        Ctx &c;
+        ~SkipGuard() { c.skip = nullptr; }
+      } guard{c};
+      c.skip = group > 1 ? &c.ctl->stop : nullptr;
+      for (int b = 0; b < group; ++b) {
+        const int jj = j + b;
+        const T *vj = V + (size_t)jj * ldv;
+        ops.precondition(c, vj, z);
+        ops.apply(c, z, w);
         ProfScope ps(c, EG_K_KRYLOV, 4);
-        cgs_passes<T>(c, N, w, V, ldv, nc, ops.mtab, ops.period, R);
-        normalize_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, w, V + (size_t)(j + 1) * ldv, c.ctl);
+        cgs_passes<T>(c, N, w, V, ldv, jj + 1, ops.mtab, ops.period, R);
+        normalize_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, w, V + (size_t)(jj + 1) * ldv, c.ctl);
         EG_CUDA(cudaGetLastError());
       }
-      EG_CUDA(cudaMemcpyAsync(&c.hctl->stop, &c.ctl->stop, 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                              c.stream));
+      c.skip = nullptr;
+      // j, count, stop and err of the control block
+      EG_CUDA(cudaMemcpyAsync(&c.hctl->j, &c.ctl->j, 4 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
       c.sync();
-      ++iterations;
       if (c.hctl->err) fail(EG_ERR_GMRES_BREAKDOWN, "GMRES Arnoldi breakdown");
-      if (c.hctl->stop) break;
+      const int done = c.hctl->count - j;  // steps completed in this group
+      iterations += done;
+      j += done;
+      if (c.hctl->stop || done < group) break;
     }
     {
       ProfScope ps(c, EG_K_KRYLOV, 2);

@@ -57,8 +57,10 @@ __global__ void add_scaled_f32_kernel(int n, double a, const float *__restrict__
 template <int Q>
 __global__ void __launch_bounds__(128)
     cell_gemv_f32_kernel(Geo g, const double *__restrict__ tab, const float *__restrict__ Xf,
-                         const double *__restrict__ Cb, const float *__restrict__ v, float *__restrict__ out) {
+                         const double *__restrict__ Cb, const float *__restrict__ v, float *__restrict__ out,
+                         const int *__restrict__ skip) {
   constexpr int P = Q * Q, M = 4 * P, T = 4 * Q;
+  if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
   __shared__ STab<Q> st;
   __shared__ float vl[4 * T], mid[M];
   load_tables<Q>(st, tab);
@@ -98,7 +100,8 @@ __global__ void __launch_bounds__(128)
 // y_f = D_f v_f - contrib[L][ls] - contrib[R][rs]
 __global__ void face_combine_f32_kernel(int nx, int ny, int T, int nl, const float *__restrict__ D,
                                         const float *__restrict__ v, const float *__restrict__ contrib,
-                                        float *__restrict__ y) {
+                                        float *__restrict__ y, const int *__restrict__ skip) {
+  if (skip != nullptr && *skip) return;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nl) return;
   const int f = idx / T, i = idx % T;
@@ -110,7 +113,8 @@ __global__ void face_combine_f32_kernel(int nx, int ny, int T, int nl, const flo
 // x_b = Inv_b b_b for column-major FP32 block inverses; one thread per row.
 __global__ void __launch_bounds__(256)
     block_gemv_f32_kernel(const float *__restrict__ inv, int nblocks, int bs, const float *__restrict__ b,
-                          float *__restrict__ x) {
+                          float *__restrict__ x, const int *__restrict__ skip) {
+  if (skip != nullptr && *skip) return;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long long)nblocks * bs) return;
   const int blk = (int)(id / bs), row = (int)(id % bs);
@@ -138,21 +142,22 @@ struct MixedHdgOps : LinearOpsT<float> {
     N = c.nl;
     mtab = c.mtab_hdg;
     period = 2 * c.t;
+    group = kArnoldiGroup;
   }
   void apply(Ctx &c, const float *x, float *y) override {
     ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
     const int grid = std::min(c.n, sm_count_mixed() * 16);
     EG_DISPATCH_Q(c.q, (cell_gemv_f32_kernel<Q><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.Xf, c.Cb, x,
-                                                                          c.contribf)));
+                                                                          c.contribf, c.skip)));
     EG_CUDA(cudaGetLastError());
     face_combine_f32_kernel<<<(c.nl + 255) / 256, 256, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.t, c.nl, c.Df, x,
-                                                                      c.contribf, y);
+                                                                      c.contribf, y, c.skip);
     EG_CUDA(cudaGetLastError());
   }
   void precondition(Ctx &c, const float *b, float *x) override {
     ProfScope ps(c, EG_K_PC_APPLY, 1);
     const long long total = (long long)c.nf * c.t;
-    block_gemv_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.pcf, c.nf, c.t, b, x);
+    block_gemv_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.pcf, c.nf, c.t, b, x, c.skip);
     EG_CUDA(cudaGetLastError());
   }
 };
