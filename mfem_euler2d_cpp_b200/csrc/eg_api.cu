@@ -652,7 +652,12 @@ int eg_download(eg_ctx *ctx, int slot, double *dst) {
         eg::download_vec(c, dst, c.pc_dg, (size_t)c.n * c.m * c.m);
       } else {
         if (!c.pc_hdg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
+        if (!dst) eg::fail(EG_ERR_INVALID, "null vector");
+        // stored row-major for the block GEMV; the slot is column-major
+        eg::launch_transpose_blocks(c, c.pc_hdg, c.nf, c.t);
         eg::download_vec(c, dst, c.pc_hdg, (size_t)c.nf * c.t * c.t);
+        eg::launch_transpose_blocks(c, c.pc_hdg, c.nf, c.t);
+        c.sync();
       }
       return;
     }

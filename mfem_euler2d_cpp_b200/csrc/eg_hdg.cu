@@ -1086,7 +1086,8 @@ __global__ void __launch_bounds__(64)
       out = Inv;
     }
     for (int i = threadIdx.x; i < T; i += blockDim.x) pivots[(size_t)f * T + i] = factor ? piv_s[i] : i;
-    for (int o = threadIdx.x; o < T * T; o += blockDim.x) blocks[(size_t)f * T * T + o] = out[o];
+    // stored row-major (one contiguous row per output of the block GEMV)
+    for (int o = threadIdx.x; o < T * T; o += blockDim.x) blocks[(size_t)f * T * T + (o % T) * T + o / T] = out[o];
   }
 }
 
@@ -1097,7 +1098,7 @@ __global__ void __launch_bounds__(64)
 // Rows never move: the pivot row of step k ends up holding row k of S^{-1}.
 // The pivot search is three warp reductions on IEEE bit patterns and the
 // normalised pivot row is broadcast by shuffles, so no step needs a barrier.
-// `pivots` receives the pivot row of every step.
+// `pivots` receives the pivot row of every step. Blocks are stored row-major.
 template <int T>
 __global__ void __launch_bounds__(128)
     schur_jacobi_warp_kernel(int nx, int ny, int nf, const double *__restrict__ D,
@@ -1120,11 +1121,11 @@ __global__ void __launch_bounds__(128)
       sr[c] = row_ok ? ((lane == c ? d : 0.) - pl[c * T + lane]) - pr[c * T + lane] : 0.;
       xr[c] = lane == c ? 1. : 0.;
     }
-    double *out = blocks + (size_t)f * T * T;
+    double *out = blocks + (size_t)f * T * T;  // row-major
     if (!factor) {
       if (row_ok) {
 #pragma unroll
-        for (int c = 0; c < T; ++c) out[c * T + lane] = sr[c];
+        for (int c = 0; c < T; ++c) out[lane * T + c] = sr[c];
         pivots[(size_t)f * T + lane] = lane;
       }
       continue;
@@ -1179,25 +1180,48 @@ __global__ void __launch_bounds__(128)
     }
     if (row_ok) {
 #pragma unroll
-      for (int c = 0; c < T; ++c) out[c * T + pos] = xr[c];
+      for (int c = 0; c < T; ++c) out[pos * T + c] = xr[c];
       pivots[(size_t)f * T + pos] = lane;
     }
   }
 }
 
-// x_b = Inv_b b_b for column-major bs x bs inverses; one thread per output row.
+// x_b = Inv_b b_b for row-major bs x bs inverses (bs even); one thread per
+// output row, which reads its row with 16-byte loads.
 __global__ void __launch_bounds__(256) block_gemv_kernel(const double *__restrict__ inv, int nblocks, int bs,
                                                          const double *__restrict__ b,
                                                          double *__restrict__ x, const int *__restrict__ skip) {
   if (skip != nullptr && *skip) return;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long long)nblocks * bs) return;
-  const int blk = (int)(id / bs), row = (int)(id % bs);
-  const double *ib = inv + (size_t)blk * bs * bs + row;
+  const int blk = (int)(id / bs);
+  const double2 *ib = reinterpret_cast<const double2 *>(inv + (size_t)id * bs);
   const double *bb = b + (size_t)blk * bs;
   double acc = 0.;
-  for (int c = 0; c < bs; ++c) acc += ib[(size_t)c * bs] * bb[c];
+  for (int c = 0; c < bs / 2; ++c) {
+    const double2 a = ib[c];
+    acc += a.x * bb[2 * c];
+    acc += a.y * bb[2 * c + 1];
+  }
   x[id] = acc;
+}
+
+// In-place transpose of every bs x bs block (one thread per pair i < j).
+__global__ void transpose_blocks_kernel(double *a, int nblocks, int bs) {
+  const long long per = (long long)bs * (bs - 1) / 2;
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= per * nblocks) return;
+  const int blk = (int)(id / per);
+  int k = (int)(id % per), i = 0;
+  while (k >= bs - 1 - i) {  // row i holds the pairs (i, i+1..bs-1)
+    k -= bs - 1 - i;
+    ++i;
+  }
+  const int j = i + 1 + k;
+  double *m = a + (size_t)blk * bs * bs;
+  const double t = m[i * bs + j];
+  m[i * bs + j] = m[j * bs + i];
+  m[j * bs + i] = t;
 }
 
 // ================================================================ launchers
@@ -1318,6 +1342,13 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er) {
   ProfScope ps(c, EG_K_RECOVERED_RESIDUAL, 1);
   EG_DISPATCH_Q(c.q, (recovered_residual_kernel<Q><<<(total + 255) / 256, 256, 0, c.stream>>>(
                          c.geo, c.tab, c.sf, c.D, eq, er)));
+  EG_CUDA(cudaGetLastError());
+}
+
+void launch_transpose_blocks(Ctx &c, double *a, int nblocks, int bs) {
+  const long long total = (long long)nblocks * bs * (bs - 1) / 2;
+  if (total == 0) return;
+  transpose_blocks_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(a, nblocks, bs);
   EG_CUDA(cudaGetLastError());
 }
 

@@ -238,6 +238,8 @@ void launch_recovered_residual(Ctx &c, const double *eq, double *er);
 void launch_schur_jacobi(Ctx &c, bool factor);
 // x = Inv b for explicit block inverses (Schur block Jacobi apply).
 void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x);
+// in-place transpose of every bs x bs block of `a`
+void launch_transpose_blocks(Ctx &c, double *a, int nblocks, int bs);
 // ---- eg_api.cu ----
 // Sets the context's description (geometry, tables, metrics) for its size.
 void upload_desc(Ctx &c, const eg_desc &d);

@@ -117,11 +117,17 @@ __global__ void __launch_bounds__(256)
   if (skip != nullptr && *skip) return;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long long)nblocks * bs) return;
-  const int blk = (int)(id / bs), row = (int)(id % bs);
-  const float *ib = inv + (size_t)blk * bs * bs + row;
+  const int blk = (int)(id / bs);
+  const float4 *ib = reinterpret_cast<const float4 *>(inv + (size_t)id * bs);  // row-major, bs % 4 == 0
   const float *bb = b + (size_t)blk * bs;
   float acc = 0.f;
-  for (int c = 0; c < bs; ++c) acc = fmaf(ib[(size_t)c * bs], bb[c], acc);
+  for (int c = 0; c < bs / 4; ++c) {
+    const float4 a = ib[c];
+    acc = fmaf(a.x, bb[4 * c], acc);
+    acc = fmaf(a.y, bb[4 * c + 1], acc);
+    acc = fmaf(a.z, bb[4 * c + 2], acc);
+    acc = fmaf(a.w, bb[4 * c + 3], acc);
+  }
   x[id] = acc;
 }
 
