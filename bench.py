@@ -79,7 +79,8 @@ def algorithmic(w):
     s = sizes(w)
     n, m, t, q, p, nu, nl, nf = s["n"], s["m"], s["t"], s["q"], s["p"], s["nu"], s["nl"], s["nf"]
     return {
-        "schur_apply": ("hbm", 8.0 * (n * m * 4 * t + 64 * n * q + 3 * nl)),
+        # k >= 4 streams the 16 panels C_s X_o of a cell, lower degrees X and C
+        "schur_apply": ("hbm", 8.0 * ((n * 16 * t * t if q >= 5 else n * m * 4 * t + 64 * n * q) + 3 * nl)),
         "recover": ("hbm", 8.0 * (n * m * 4 * t + n * m + nl + nu)),
         "dg_apply": ("hbm", 8.0 * (2 * nu + 32 * n * p + 32 * nf * q)),
         "residual": ("hbm", 8.0 * (3 * nu + 6 * nf * q)),

@@ -127,7 +127,7 @@ void Ctx::ensure_hdg() {
   Cb = alloc_n<double>((size_t)n * 4 * q * 16);
   sf = alloc_n<double>((size_t)n * 4 * q);
   contrib = alloc_n<double>((size_t)n * 4 * t);
-  panels = alloc_n<double>((size_t)n * 4 * t * t);
+  panels = alloc_n<double>((size_t)n * (schur_panels_full(q) ? 16 : 4) * t * t);
   rhs = alloc_n<double>(nl);
   lam = alloc_n<double>(nl);
   tmp_trace = alloc_n<double>(nl);

@@ -171,7 +171,8 @@ long long estimate_bytes(const eg_request &r) {
   const long long nu = n * m, nl = nf * t, N = std::max(nu, nl), R = 20;
   long long d = 14 * nu + 5 * nf * q + N * (R + 1) + 6 * N + 2 * nl;
   if (r.form == EG_FORM_HDG) {
-    d += n * m * (4 * t + 1) + n * 4 * q * 17 + n * 4 * t + n * 4 * t * t + 4 * nl + nf * t * t + nf * t / 2;
+    d += n * m * (4 * t + 1) + n * 4 * q * 17 + n * 4 * t + n * (q >= 5 ? 16 : 4) * t * t + 4 * nl + nf * t * t +
+         nf * t / 2;
     if (r.precision == EG_PRECISION_MIXED) d += (n * m * 4 * t + nf * t * t + nl * (R + 9) + n * 4 * t) / 2;
     if (r.precond == EG_PC_BLOCK_ILU0) d += 8 * nf * t * t + n * 16 * t * t;
   } else {

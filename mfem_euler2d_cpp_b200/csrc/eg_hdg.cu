@@ -142,11 +142,14 @@ __device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, 
     contrib[(size_t)e * 4 * T + o] = res;
   }
   if (panels) {
-    for (int o = threadIdx.x; o < 4 * T * T; o += blockDim.x) {
-      const int s = o / (T * T), rem = o % (T * T);
+    // the 4 diagonal panels, or all 16 ([s][o]) where the Schur action uses them
+    constexpr int NPAN = schur_panels_full(Q) ? 16 : 4;
+    for (int o = threadIdx.x; o < NPAN * T * T; o += blockDim.x) {
+      const int pan = o / (T * T), rem = o % (T * T);
+      const int s = NPAN == 16 ? pan >> 2 : pan, so = NPAN == 16 ? pan & 3 : pan;
       const int row = rem % T, cc = rem / T;
       const int jj = row >> 2, c = row & 3;
-      const double *xc = R + (size_t)(s * T + cc) * M;
+      const double *xc = R + (size_t)(so * T + cc) * M;
       double val[4] = {0., 0., 0., 0.};
       for (int l = 0; l < Q; ++l) {
         const double f = st.fb(s, jj, l);
@@ -158,7 +161,7 @@ __device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, 
       double res = 0.;
 #pragma unroll
       for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
-      panels[(size_t)e * 4 * T * T + o] = res;
+      panels[(size_t)e * NPAN * T * T + o] = res;
     }
   }
 }
@@ -1007,6 +1010,35 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// Schur action from the 16 panels of a cell (degrees with
+// schur_panels_full): contrib[e][s] = sum_o (C_s X_o) v_o, the same product as
+// the C restriction of X v (src/operators.cpp:166-178) with the C X panels
+// formed once per condensation, so that each apply streams 16 t^2 doubles per
+// cell instead of m x 4t. One thread per output (s, row); consecutive rows
+// read consecutive panel entries.
+template <int Q>
+__global__ void __launch_bounds__(((16 * Q + 31) / 32) * 32)
+    panel_gemv_kernel(Geo g, const double *__restrict__ panels, const double *__restrict__ v,
+                      double *__restrict__ out, const int *__restrict__ skip) {
+  constexpr int T = 4 * Q, TT = T * T;
+  if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
+  __shared__ double vl[4 * T];
+  const int o = threadIdx.x, s = o / T, row = o % T;
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * T; i += blockDim.x)
+      vl[i] = v[(size_t)cell_face(e, i / T, g.nx, g.ny) * T + (i % T)];
+    __syncthreads();
+    if (o < 4 * T) {
+      const double *P = panels + ((size_t)e * 16 + s * 4) * TT + row;
+      double acc = 0.;
+#pragma unroll 8
+      for (int k = 0; k < 4 * T; ++k) acc += P[(size_t)(k / T) * TT + (k % T) * T] * vl[k];
+      out[(size_t)e * 4 * T + o] = acc;
+    }
+  }
+}
+
 // y_f = D_f v_f - contrib[L][ls] - contrib[R][rs]  (one thread per trace dof)
 __global__ void face_combine_kernel(int nx, int ny, int T, int nl, const double *__restrict__ D,
                                     const double *__restrict__ v, const double *__restrict__ contrib,
@@ -1070,8 +1102,11 @@ __global__ void __launch_bounds__(64)
     __syncthreads();
     const int L = f >> 1, ls = (f & 1) ? 3 : 1;
     const int R = neighbour(L, ls, nx, ny), rs = ls - 1;
-    const double *pl = panels + ((size_t)L * 4 + ls) * T * T;
-    const double *pr = panels + ((size_t)R * 4 + rs) * T * T;
+    // diagonal panels C_s X_s of the two cells (16 panels per cell where the
+    // Schur action keeps them all)
+    constexpr bool kFull = schur_panels_full(T / 4);
+    const double *pl = panels + (kFull ? (size_t)L * 16 + ls * 5 : (size_t)L * 4 + ls) * T * T;
+    const double *pr = panels + (kFull ? (size_t)R * 16 + rs * 5 : (size_t)R * 4 + rs) * T * T;
     for (int o = threadIdx.x; o < T * T; o += blockDim.x) {
       const int row = o % T, col = o / T;
       const double d = row == col ? D[(size_t)f * T + row] : 0.;
@@ -1111,8 +1146,11 @@ __global__ void __launch_bounds__(128)
   for (int f = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); f < nf; f += nwarps) {
     const int L = f >> 1, ls = (f & 1) ? 3 : 1;
     const int R = neighbour(L, ls, nx, ny), rs = ls - 1;
-    const double *pl = panels + ((size_t)L * 4 + ls) * T * T;
-    const double *pr = panels + ((size_t)R * 4 + rs) * T * T;
+    // diagonal panels C_s X_s of the two cells (16 panels per cell where the
+    // Schur action keeps them all)
+    constexpr bool kFull = schur_panels_full(T / 4);
+    const double *pl = panels + (kFull ? (size_t)L * 16 + ls * 5 : (size_t)L * 4 + ls) * T * T;
+    const double *pr = panels + (kFull ? (size_t)R * 16 + rs * 5 : (size_t)R * 4 + rs) * T * T;
     const bool row_ok = lane < T;
     const double d = row_ok ? D[(size_t)f * T + lane] : 0.;
     double sr[T], xr[T];
@@ -1320,8 +1358,22 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
 void launch_schur_apply(Ctx &c, const double *v, double *y) {
   ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
   const int grid = std::min(c.n, sm_count_hdg() * 16);
-  EG_DISPATCH_Q(c.q, (cell_gemv_kernel<Q, false><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb,
-                                                                            v, c.contrib, c.skip)));
+  if (schur_panels_full(c.q)) {
+    switch (c.q) {
+#define EG_PG(QQ)                                                                                          \
+  case QQ:                                                                                                 \
+    panel_gemv_kernel<QQ><<<grid, ((16 * QQ + 31) / 32) * 32, 0, c.stream>>>(c.geo, c.panels, v, c.contrib, \
+                                                                            c.skip);                       \
+    break;
+      EG_PG(5) EG_PG(6) EG_PG(7) EG_PG(8) EG_PG(9)
+#undef EG_PG
+      default:
+        fail(EG_ERR_INVALID, "unsupported degree");
+    }
+  } else {
+    EG_DISPATCH_Q(c.q, (cell_gemv_kernel<Q, false><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb,
+                                                                              v, c.contrib, c.skip)));
+  }
   EG_CUDA(cudaGetLastError());
   const int blocks = (c.nl + 255) / 256;
   face_combine_kernel<<<blocks, 256, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.t, c.nl, c.D, v,

@@ -737,7 +737,9 @@ void build_plan(Ctx &c, int form) {
   P.data = c.alloc_n<double>((size_t)P.nnzb * BB);
   P.dinv = c.alloc_n<double>((size_t)P.rows * BB);
   P.w = c.alloc_n<double>((size_t)P.rows * P.B);
-  if (hdg) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
+  // the condensation keeps all 16 panels per cell where the Schur action
+  // streams them (same layout and arithmetic); otherwise the fill forms them
+  if (hdg && !schur_panels_full(c.q)) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
   if (!P.staged) P.work = c.alloc_n<double>((size_t)G * 3 * BB);
   P.progress = c.alloc_n<unsigned long long>(G);
   EG_CUDA(cudaMemsetAsync(P.progress, 0, sizeof(unsigned long long) * G, c.stream));
@@ -846,14 +848,17 @@ void ilu_refresh(Ctx &c, int form, bool factor) {
   EG_CUDA(cudaMemsetAsync(P.abort, 0, sizeof(int), c.stream));
   const int sms = sm_count_ilu();
   if (hdg) {
-    const long long np = (long long)c.n * 16 * c.t * c.t;
-    const int grid = (int)std::min<long long>((np + 255) / 256, (long long)sms * 16);
-    EG_DISPATCH_Q(c.q, (ilu_panels_kernel<Q><<<grid, 256, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb, P.panels16)));
-    EG_CUDA(cudaGetLastError());
+    const double *pan16 = schur_panels_full(c.q) ? c.panels : P.panels16;
+    if (!schur_panels_full(c.q)) {
+      const long long np = (long long)c.n * 16 * c.t * c.t;
+      const int grid = (int)std::min<long long>((np + 255) / 256, (long long)sms * 16);
+      EG_DISPATCH_Q(c.q, (ilu_panels_kernel<Q><<<grid, 256, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb, P.panels16)));
+      EG_CUDA(cudaGetLastError());
+    }
     const long long ne = (long long)P.nnzb * c.t * c.t;
     const int g2 = (int)std::min<long long>((ne + 255) / 256, (long long)sms * 16);
     ilu_fill_hdg_kernel<<<g2, 256, 0, c.stream>>>(P.nnzb, c.t, P.erow, P.col, P.fill_ptr, P.fill_src, c.D,
-                                                  P.panels16, P.data);
+                                                  pan16, P.data);
   } else {
     const int grid = std::min(P.nnzb, sms * 8);
     EG_DISPATCH_Q(c.q, (ilu_fill_dg_kernel<Q><<<grid, 256, 0, c.stream>>>(

@@ -105,6 +105,9 @@ using LinearOps = LinearOpsT<double>;
 // kernels honour Ctx::skip: a group costs at most kArnoldiGroup - 1 steps of
 // no-op launches after convergence and saves a host round trip per step.
 constexpr int kArnoldiGroup = 4;
+// Degrees whose Schur action streams the 16 panels C_s X_o of a cell (16 t^2
+// doubles) instead of X (m x 4t): fewer bytes from q = 5 (k = 4) on.
+__host__ __device__ constexpr bool schur_panels_full(int q) { return q >= 5; }
 
 // Krylov workspace of one vector type: basis (R+1 columns, leading dimension
 // ld) and the work vectors of the solver.
@@ -164,7 +167,10 @@ struct Ctx {
   double *Cb = nullptr;    // n*4q*16 restriction flux blocks C
   double *sf = nullptr;    // n*4q lift scalars B
   double *contrib = nullptr;  // n*4t per-cell face contributions
-  double *panels = nullptr;   // n*4*t*t Schur Jacobi panels
+  // Schur panels C_s X_o of every cell, column-major t x t: the 4 diagonal
+  // ones (s = o, the Jacobi blocks) or, where schur_panels_full(q), all 16
+  // ([cell][s][o]), which the Schur action then streams instead of X
+  double *panels = nullptr;
   double *rhs = nullptr, *lam = nullptr, *tmp_trace = nullptr;  // nl
   double *work_cell = nullptr;  // global LU workspace for large cells
   int work_slots = 0;
