@@ -58,8 +58,8 @@ K_NAMES = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "reco
 
 # DRAM bytes (read + write) per cell of one launch, from one ncu capture of the
 # kernel on a 64x64 mesh of the same degree (profiles/condense_gj_q4_64x64.txt,
-# profiles/cell_gemv_q4_64x64.txt); per-launch traffic grows with the cell count.
-NCU_TRAFFIC_PER_CELL = {("condense", 4): 288.21e6 / 4096, ("schur_apply", 4): 279.9e6 / 4096}
+# profiles/panel_gemv_q4_64x64.txt); per-launch traffic grows with the cell count.
+NCU_TRAFFIC_PER_CELL = {("condense", 4): 444.54e6 / 4096, ("schur_apply", 4): 216.24e6 / 4096}
 
 
 def traffic(name, w):
