@@ -205,6 +205,8 @@ struct Ctx {
   double *step_bufs = nullptr;  // time loop: step state, stage base, 4 slopes (6 nu), reused
   // mixed precision: FP32 copies of X, of the Schur block-Jacobi inverses and
   // of D, and the FP32 Krylov workspace of the inner Schur solve
+  // mixed precision: Xf is the FP32 copy of X, or of the 16 Schur panels per
+  // cell where schur_panels_full(q)
   float *Xf = nullptr, *pcf = nullptr, *Df = nullptr, *contribf = nullptr;
   float *kfV = nullptr, *kfw = nullptr, *kfz = nullptr, *kfres = nullptr, *kfcomb = nullptr,
         *kfcorr = nullptr, *kfx = nullptr, *kfrhs = nullptr;

@@ -97,6 +97,31 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// FP32 Schur action from FP32 copies of the 16 panels C_s X_o of a cell
+// (degrees with schur_panels_full; the FP64 panel form is panel_gemv_kernel).
+template <int Q>
+__global__ void __launch_bounds__(((16 * Q + 31) / 32) * 32)
+    panel_gemv_f32_kernel(Geo g, const float *__restrict__ panels, const float *__restrict__ v,
+                          float *__restrict__ out, const int *__restrict__ skip) {
+  constexpr int T = 4 * Q, TT = T * T;
+  if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
+  __shared__ float vl[4 * T];
+  const int o = threadIdx.x, s = o / T, row = o % T;
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * T; i += blockDim.x)
+      vl[i] = v[(size_t)cell_face(e, i / T, g.nx, g.ny) * T + (i % T)];
+    __syncthreads();
+    if (o < 4 * T) {
+      const float *P = panels + ((size_t)e * 16 + s * 4) * TT + row;
+      float acc = 0.f;
+#pragma unroll 8
+      for (int k = 0; k < 4 * T; ++k) acc = fmaf(P[(size_t)(k / T) * TT + (k % T) * T], vl[k], acc);
+      out[(size_t)e * 4 * T + o] = acc;
+    }
+  }
+}
+
 // y_f = D_f v_f - contrib[L][ls] - contrib[R][rs]
 __global__ void face_combine_f32_kernel(int nx, int ny, int T, int nl, const float *__restrict__ D,
                                         const float *__restrict__ v, const float *__restrict__ contrib,
@@ -153,8 +178,22 @@ struct MixedHdgOps : LinearOpsT<float> {
   void apply(Ctx &c, const float *x, float *y) override {
     ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
     const int grid = std::min(c.n, sm_count_mixed() * 16);
-    EG_DISPATCH_Q(c.q, (cell_gemv_f32_kernel<Q><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.Xf, c.Cb, x,
-                                                                          c.contribf, c.skip)));
+    if (schur_panels_full(c.q)) {  // Xf holds the FP32 panels
+      switch (c.q) {
+#define EG_PGF(QQ)                                                                                    \
+  case QQ:                                                                                            \
+    panel_gemv_f32_kernel<QQ><<<grid, ((16 * QQ + 31) / 32) * 32, 0, c.stream>>>(c.geo, c.Xf, x, c.contribf, \
+                                                                                c.skip);              \
+    break;
+        EG_PGF(5) EG_PGF(6) EG_PGF(7) EG_PGF(8) EG_PGF(9)
+#undef EG_PGF
+        default:
+          fail(EG_ERR_INVALID, "unsupported degree");
+      }
+    } else {
+      EG_DISPATCH_Q(c.q, (cell_gemv_f32_kernel<Q><<<grid, 128, 0, c.stream>>>(c.geo, c.tab, c.Xf, c.Cb, x,
+                                                                            c.contribf, c.skip)));
+    }
     EG_CUDA(cudaGetLastError());
     face_combine_f32_kernel<<<(c.nl + 255) / 256, 256, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.t, c.nl, c.Df, x,
                                                                       c.contribf, y, c.skip);
@@ -171,7 +210,9 @@ struct MixedHdgOps : LinearOpsT<float> {
 void ensure_mixed(Ctx &c) {
   if (c.Xf) return;
   c.ensure_krylov();  // fixes the restart length both solvers use
-  c.Xf = c.alloc_n<float>((size_t)c.n * c.m * 4 * c.t);
+  // FP32 copy of X, or of the 16 Schur panels per cell where the FP64 Schur
+  // action streams those (schur_panels_full)
+  c.Xf = c.alloc_n<float>((size_t)c.n * (schur_panels_full(c.q) ? 16 * c.t * c.t : c.m * 4 * c.t));
   c.pcf = c.alloc_n<float>((size_t)c.nf * c.t * c.t);
   c.Df = c.alloc_n<float>(c.nl);
   c.contribf = c.alloc_n<float>((size_t)c.n * 4 * c.t);
@@ -191,8 +232,13 @@ void ensure_mixed(Ctx &c) {
 void mixed_prepare(Ctx &c) {
   ensure_mixed(c);
   ProfScope ps(c, EG_K_VECTOR, 3);
-  const long long nx = (long long)c.n * c.m * 4 * c.t;
-  x_to_f32_kernel<<<vgrid(nx), 256, 0, c.stream>>>(c.n, c.m, 4 * c.t + 1, c.XY, c.Xf);
+  if (schur_panels_full(c.q)) {
+    const long long npan = (long long)c.n * 16 * c.t * c.t;
+    to_f32_kernel<<<vgrid(npan), 256, 0, c.stream>>>(npan, c.panels, c.Xf);
+  } else {
+    const long long nx = (long long)c.n * c.m * 4 * c.t;
+    x_to_f32_kernel<<<vgrid(nx), 256, 0, c.stream>>>(c.n, c.m, 4 * c.t + 1, c.XY, c.Xf);
+  }
   const long long np = (long long)c.nf * c.t * c.t;
   to_f32_kernel<<<vgrid(np), 256, 0, c.stream>>>(np, c.pc_hdg, c.pcf);
   to_f32_kernel<<<vgrid(c.nl), 256, 0, c.stream>>>(c.nl, c.D, c.Df);
