@@ -368,11 +368,22 @@ def run_ours(args, world, rank, local):
         extd = torch.cuda.ExternalStream(ctxd.stream_ptr())
         for _ in range(W):
             std.next()
+        ctxd.lib.eg_profile_reset(ctxd.h)
+        ctxd.lib.eg_profile_enable(ctxd.h, 1)
         dg_ms, dg_dev = timed_updates(ctxd, std, K, world, extd)
+        dg_kry = timed_updates.krylov
+        dg_prof = {}
+        for i, name in enumerate(K_NAMES):
+            import ctypes as C
+
+            ms, cnt = C.c_double(), C.c_longlong()
+            ctxd.lib.eg_profile_query(ctxd.h, i, C.byref(ms), C.byref(cnt))
+            if cnt.value:
+                dg_prof[name] = round(ms.value / K, 3)
         dg_ms = max_over_ranks(world, dg_ms)
         dg = {"value": dg_ms * 1e-3 / (K * world), "unit": "s", "ms_per_step": dg_ms / K,
               "mean_newton_device_s": dg_dev * 1e-3 / K, "form": "dg",
-              "krylov_per_update": timed_updates.krylov / K}
+              "krylov_per_update": dg_kry / K, "kernel_ms_per_update": dg_prof}
         std.close()
         ctxd.close()
 
