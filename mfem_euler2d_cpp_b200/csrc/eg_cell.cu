@@ -285,6 +285,80 @@ __global__ void __launch_bounds__(256) block_apply_kernel(const double *__restri
   for (int i = lane; i < bs; i += 32) x[(size_t)blk * bs + i] = v[i];
 }
 
+// The same apply with the block's part of x in registers (lane holds rows
+// lane + 32 r, r < R): sweep steps communicate through shuffles only, so the
+// loads of later factor columns, which do not depend on x, are issued ahead
+// of the arithmetic (unrolled column loops) instead of exposing one global
+// latency per step. The diagonal is applied as a product with its
+// reciprocal, formed off the dependency chain.
+template <int R>
+__global__ void __launch_bounds__(256) block_apply_reg_kernel(const double *__restrict__ blocks,
+                                                              const int *__restrict__ piv, int nblocks,
+                                                              int m, const double *__restrict__ b,
+                                                              double *__restrict__ x) {
+  extern __shared__ double xs[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int blk = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (blk >= nblocks) return;
+  double *v = xs + (size_t)warp * m;
+  const double *lu = blocks + (size_t)blk * m * m;
+  const int *pv = piv + (size_t)blk * m;
+  for (int i = lane; i < m; i += 32) v[i] = b[(size_t)blk * m + i];
+  __syncwarp();
+  if (lane == 0)
+    for (int i = 0; i < m; ++i) {  // row exchanges of the factorisation, in order
+      const int p = pv[i];
+      if (p != i) {
+        const double t = v[i];
+        v[i] = v[p];
+        v[p] = t;
+      }
+    }
+  __syncwarp();
+  double xr[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) xr[r] = lane + 32 * r < m ? v[lane + 32 * r] : 0.;
+  // forward: unit lower triangle
+#pragma unroll
+  for (int jb = 0; jb < R; ++jb) {
+#pragma unroll 8
+    for (int jl = 0; jl < 32; ++jl) {
+      const int j = 32 * jb + jl;
+      if (j < m) {
+        const double xj = __shfl_sync(0xffffffffu, xr[jb], jl);
+        const double *col = lu + (size_t)j * m;
+#pragma unroll
+        for (int r = jb; r < R; ++r) {
+          const int i = lane + 32 * r;
+          if (i > j && i < m) xr[r] -= col[i] * xj;
+        }
+      }
+    }
+  }
+  // backward: upper triangle with its diagonal
+#pragma unroll
+  for (int jb = R - 1; jb >= 0; --jb) {
+#pragma unroll 8
+    for (int jl = 31; jl >= 0; --jl) {
+      const int j = 32 * jb + jl;
+      if (j < m) {
+        const double *col = lu + (size_t)j * m;
+        const double rd = 1.0 / col[j];
+        const double xo = __shfl_sync(0xffffffffu, xr[jb], jl) * rd;
+        if (lane == jl) xr[jb] = xo;
+#pragma unroll
+        for (int r = 0; r <= jb; ++r) {
+          const int i = lane + 32 * r;
+          if (i < j) xr[r] -= col[i] * xo;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (lane + 32 * r < m) x[(size_t)blk * m + lane + 32 * r] = xr[r];
+}
+
 // ================================================================ launchers
 static Frozen frozen_of(Ctx &c) { return Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}; }
 
@@ -371,7 +445,16 @@ void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblock
   const int grid = (nblocks + warps - 1) / warps;
   const size_t dyn = sizeof(double) * bs * warps;
   ProfScope ps(c, EG_K_PC_APPLY, 1);
-  block_apply_kernel<<<grid, warps * 32, dyn, c.stream>>>(blocks, piv, nblocks, bs, b, x);
+  switch ((bs + 31) / 32) {
+#define EG_BAR(RR)                                                                                    \
+  case RR:                                                                                            \
+    block_apply_reg_kernel<RR><<<grid, warps * 32, dyn, c.stream>>>(blocks, piv, nblocks, bs, b, x);   \
+    break;
+    EG_BAR(1) EG_BAR(2) EG_BAR(4) EG_BAR(5) EG_BAR(7) EG_BAR(8) EG_BAR(11)
+#undef EG_BAR
+    default:
+      block_apply_kernel<<<grid, warps * 32, dyn, c.stream>>>(blocks, piv, nblocks, bs, b, x);
+  }
   EG_CUDA(cudaGetLastError());
 }
 
