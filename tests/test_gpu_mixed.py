@@ -1,6 +1,7 @@
 """Mixed precision on the condensed HDG solve: an FP32 inner GMRES with FP32
-block-Jacobi and an FP32 copy of X, inside FP64 iterative refinement that
-stops at the FP64 solver's own relative residual (1e-12 here).
+block-Jacobi and an FP32 copy of X (k <= 3) or of the 16 Schur panels C_s X_o
+per cell (k >= 4), inside FP64 iterative refinement that stops at the FP64
+solver's own relative residual (1e-12 here).
 
 Because every linear solve still meets the reference's residual bound, the
 results are checked against the reference's FP64 outputs: the Schur solution
@@ -63,12 +64,13 @@ def test_mixed_cli_matches_reference(tmp_path):
         assert row["precision"] == "mixed"
 
 
-def test_mixed_matches_fp64_on_a_larger_mesh():
-    """48x48 Q3, one SSP-DIRK3 step with 3 updates per stage: mixed against the
-    FP64 engine on the same schedule."""
+@pytest.mark.parametrize("n,k", [(48, 3), (32, 4)], ids=["48x48_k3_X", "32x32_k4_panels"])
+def test_mixed_matches_fp64_on_a_larger_mesh(n, k):
+    """One SSP-DIRK3 step with 3 updates per stage: mixed against the FP64
+    engine on the same schedule (k = 3 streams X, k = 4 the Schur panels)."""
     out = {}
     for prec in (capi.PRECISION_FP64, capi.PRECISION_MIXED):
-        d = capi.simple_wave_desc(48, 48, 3, 40.0)
+        d = capi.simple_wave_desc(n, n, k, 40.0)
         with capi.Context(d, capi.default_opts(form=capi.FORM_HDG, precision=prec)) as ctx:
             ro, keep = capi.run_options(integrator="ssp-dirk3", steps=1, newton_steps=3, cfl=1.0,
                                         form_name="hdg", precond_name="block-jacobi")
