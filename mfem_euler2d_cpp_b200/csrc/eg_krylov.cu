@@ -421,16 +421,37 @@ void launch_fill(Ctx &c, int N, double v, double *out) {
   EG_CUDA(cudaGetLastError());
 }
 
+// CTAs of KERN (kCgsThreads each) resident at once on the device: one wave.
+// Queried once per kernel; a property of the kernel and the device only.
+template <auto KERN>
+int cgs_wave() {
+  static const int wave = [] {
+    int per_sm = 0, dev = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERN, kCgsThreads, 0) != cudaSuccess) per_sm = 1;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sms = 148;
+    cudaGetLastError();
+    return std::max(1, per_sm) * std::max(1, sms);
+  }();
+  return wave;
+}
+
 // The three CGS2 passes of Arnoldi step j (src/linear.cpp:104-118).
 template <class T, int NC>
 void cgs_reg_passes(Ctx &c, int N, T *w, const T *V, size_t ldv, int nc, const double *mtab, int period, int R) {
-  const int grid = cgs_grid(N);
-  cgs_reg_kernel<0, T, NC><<<grid, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
-                                                                     c.counter, c.ctl, R);
-  cgs_reg_kernel<1, T, NC><<<grid, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
-                                                                     c.counter, c.ctl, R);
-  cgs_reg_kernel<2, T, NC><<<grid, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
-                                                                     c.counter, c.ctl, R);
+  // each pass at most one wave of resident CTAs (the passes differ in
+  // registers); the grid depends on N and the device only, so the summation
+  // order stays fixed
+  const int g0 = std::min(cgs_grid(N), cgs_wave<cgs_reg_kernel<0, T, NC>>());
+  const int g1 = std::min(cgs_grid(N), cgs_wave<cgs_reg_kernel<1, T, NC>>());
+  const int g2 = std::min(cgs_grid(N), cgs_wave<cgs_reg_kernel<2, T, NC>>());
+  cgs_reg_kernel<0, T, NC><<<g0, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                                   c.counter, c.ctl, R);
+  cgs_reg_kernel<1, T, NC><<<g1, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                                   c.counter, c.ctl, R);
+  cgs_reg_kernel<2, T, NC><<<g2, kCgsThreads, 0, c.stream>>>(N, w, V, ldv, nc, mtab, period, c.partials,
+                                                                   c.counter, c.ctl, R);
 }
 template <class T>
 void cgs_passes(Ctx &c, int N, T *w, const T *V, size_t ldv, int nc, const double *mtab, int period, int R) {
