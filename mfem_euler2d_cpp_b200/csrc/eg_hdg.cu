@@ -1225,18 +1225,23 @@ __global__ void __launch_bounds__(128)
 }
 
 // x_b = Inv_b b_b for row-major bs x bs inverses (bs even); one thread per
-// output row, which reads its row with 16-byte loads.
-__global__ void __launch_bounds__(256) block_gemv_kernel(const double *__restrict__ inv, int nblocks, int bs,
+// output row, which reads its row with 16-byte loads. BS > 0 fixes the block
+// size at compile time, so the row loop unrolls and all of a row's loads are
+// in flight together (BS = 0: any even size).
+template <int BS>
+__global__ void __launch_bounds__(256) block_gemv_kernel(const double *__restrict__ inv, int nblocks, int bs_rt,
                                                          const double *__restrict__ b,
                                                          double *__restrict__ x, const int *__restrict__ skip) {
   if (skip != nullptr && *skip) return;
+  const int bs = BS > 0 ? BS : bs_rt;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long long)nblocks * bs) return;
   const int blk = (int)(id / bs);
   const double2 *ib = reinterpret_cast<const double2 *>(inv + (size_t)id * bs);
   const double *bb = b + (size_t)blk * bs;
   double acc = 0.;
-  for (int c = 0; c < bs / 2; ++c) {
+#pragma unroll
+  for (int c = 0; c < (BS > 0 ? BS / 2 : bs / 2); ++c) {
     const double2 a = ib[c];
     acc += a.x * bb[2 * c];
     acc += a.y * bb[2 * c + 1];
@@ -1407,7 +1412,17 @@ void launch_transpose_blocks(Ctx &c, double *a, int nblocks, int bs) {
 void launch_block_inverse_apply(Ctx &c, const double *inv, int nblocks, int bs, const double *b, double *x) {
   ProfScope ps(c, EG_K_PC_APPLY, 1);
   const long long total = (long long)nblocks * bs;
-  block_gemv_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(inv, nblocks, bs, b, x, c.skip);
+  const unsigned grid = (unsigned)((total + 255) / 256);
+  switch (bs) {
+#define EG_BG(BB)                                                                                  \
+  case BB:                                                                                         \
+    block_gemv_kernel<BB><<<grid, 256, 0, c.stream>>>(inv, nblocks, bs, b, x, c.skip);             \
+    break;
+    EG_BG(4) EG_BG(8) EG_BG(12) EG_BG(16) EG_BG(20) EG_BG(24) EG_BG(28) EG_BG(32) EG_BG(36)
+#undef EG_BG
+    default:
+      block_gemv_kernel<0><<<grid, 256, 0, c.stream>>>(inv, nblocks, bs, b, x, c.skip);
+  }
   EG_CUDA(cudaGetLastError());
 }
 

@@ -135,18 +135,22 @@ __global__ void face_combine_f32_kernel(int nx, int ny, int T, int nl, const flo
   y[idx] = (D[idx] * v[idx] - contrib[(size_t)L * 4 * T + ls * T + i]) - contrib[(size_t)R * 4 * T + rs * T + i];
 }
 
-// x_b = Inv_b b_b for column-major FP32 block inverses; one thread per row.
+// x_b = Inv_b b_b for row-major FP32 block inverses; one thread per row (BS > 0:
+// compile-time block size, the row loop unrolls; BS = 0: any multiple of 4).
+template <int BS>
 __global__ void __launch_bounds__(256)
-    block_gemv_f32_kernel(const float *__restrict__ inv, int nblocks, int bs, const float *__restrict__ b,
+    block_gemv_f32_kernel(const float *__restrict__ inv, int nblocks, int bs_rt, const float *__restrict__ b,
                           float *__restrict__ x, const int *__restrict__ skip) {
   if (skip != nullptr && *skip) return;
+  const int bs = BS > 0 ? BS : bs_rt;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= (long long)nblocks * bs) return;
   const int blk = (int)(id / bs);
   const float4 *ib = reinterpret_cast<const float4 *>(inv + (size_t)id * bs);  // row-major, bs % 4 == 0
   const float *bb = b + (size_t)blk * bs;
   float acc = 0.f;
-  for (int c = 0; c < bs / 4; ++c) {
+#pragma unroll
+  for (int c = 0; c < (BS > 0 ? BS / 4 : bs / 4); ++c) {
     const float4 a = ib[c];
     acc = fmaf(a.x, bb[4 * c], acc);
     acc = fmaf(a.y, bb[4 * c + 1], acc);
@@ -202,7 +206,17 @@ struct MixedHdgOps : LinearOpsT<float> {
   void precondition(Ctx &c, const float *b, float *x) override {
     ProfScope ps(c, EG_K_PC_APPLY, 1);
     const long long total = (long long)c.nf * c.t;
-    block_gemv_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(c.pcf, c.nf, c.t, b, x, c.skip);
+    const unsigned grid = (unsigned)((total + 255) / 256);
+    switch (c.t) {
+#define EG_BGF(BB)                                                                              \
+  case BB:                                                                                      \
+    block_gemv_f32_kernel<BB><<<grid, 256, 0, c.stream>>>(c.pcf, c.nf, c.t, b, x, c.skip);       \
+    break;
+      EG_BGF(4) EG_BGF(8) EG_BGF(12) EG_BGF(16) EG_BGF(20) EG_BGF(24) EG_BGF(28) EG_BGF(32) EG_BGF(36)
+#undef EG_BGF
+      default:
+        block_gemv_f32_kernel<0><<<grid, 256, 0, c.stream>>>(c.pcf, c.nf, c.t, b, x, c.skip);
+    }
     EG_CUDA(cudaGetLastError());
   }
 };
