@@ -242,7 +242,7 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
       if (refresh) mixed_prepare(c);
       res = schur_refine_mixed(c, rhs, x, refresh, tol, c.opts.max_krylov, rhs_norm, &count);
     } else {
-      res = gmres(c, ops, rhs, x, tol, c.opts.max_krylov, refresh, &count, nullptr);
+      res = gmres(c, ops, rhs, x, tol, c.opts.max_krylov, refresh, &count, nullptr, rhs_norm);
     }
   } catch (const Failure &) {
     c.check_device_error();  // a preconditioner failure on the device explains the breakdown

@@ -274,8 +274,10 @@ void launch_fill(Ctx &c, int N, double v, double *out);
 double cell_norm(Ctx &c, const double *x);
 // Weighted restarted GMRES (src/linear.cpp:76-157). Returns the true residual
 // norm; sets *count. Throws Failure on breakdown / limit / non-finite.
+// known_rhs_norm >= 0 is the caller's weighted norm of rhs (saves a reduction
+// and a host round trip).
 double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
-             bool zero_guess, int *count, double *rhs_norm_out);
+             bool zero_guess, int *count, double *rhs_norm_out, double known_rhs_norm = -1.);
 // The same iteration on FP32 vectors from a zero guess; returns the residual
 // norm reached without requiring convergence (inner solve of mixed precision).
 double gmres_f32(Ctx &c, LinearOpsT<float> &ops, const KrylovBufs<float> &kb, const float *rhs, float *x,

@@ -479,7 +479,8 @@ void cgs_passes(Ctx &c, int N, T *w, const T *V, size_t ldv, int nc, const doubl
 // Givens and all sums are FP64.
 template <class T>
 double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs, T *x, double tol, int limit,
-               bool zero_guess, bool require_converged, int *count, double *rhs_norm_out) {
+               bool zero_guess, bool require_converged, int *count, double *rhs_norm_out,
+               double known_rhs_norm) {
   const int N = ops.N;
   const int R = std::min(N, kb.R);
   const size_t ldv = kb.ld;
@@ -497,12 +498,13 @@ double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs
     sub_kernel<T><<<vec_grid(N), 256, 0, c.stream>>>(N, rhs, w, res);
     EG_CUDA(cudaGetLastError());
   }
-  const double rhs_norm = wnorm_t(c, rhs, N, ops.mtab, ops.period);
+  const double rhs_norm = known_rhs_norm >= 0. ? known_rhs_norm : wnorm_t(c, rhs, N, ops.mtab, ops.period);
   if (rhs_norm_out) *rhs_norm_out = rhs_norm;
   *count = 0;
   if (rhs_norm == 0.) return 0.;
   int iterations = 0;
-  double residual_norm = wnorm_t(c, res, N, ops.mtab, ops.period);
+  // from a zero guess the residual is a copy of rhs: the same reduction result
+  double residual_norm = zero_guess ? rhs_norm : wnorm_t(c, res, N, ops.mtab, ops.period);
   while (iterations < limit) {
     const double beta = residual_norm;
     if (beta <= tol * rhs_norm) break;
@@ -571,15 +573,15 @@ double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs
 }
 
 double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
-             bool zero_guess, int *count, double *rhs_norm_out) {
+             bool zero_guess, int *count, double *rhs_norm_out, double known_rhs_norm) {
   c.ensure_krylov();
   const KrylovBufs<double> kb{c.V, c.kw, c.kz, c.kres, c.kcomb, c.kcorr, (size_t)c.kN, c.kR};
-  return gmres_t<double>(c, ops, kb, rhs, x, tol, limit, zero_guess, true, count, rhs_norm_out);
+  return gmres_t<double>(c, ops, kb, rhs, x, tol, limit, zero_guess, true, count, rhs_norm_out, known_rhs_norm);
 }
 
 double gmres_f32(Ctx &c, LinearOpsT<float> &ops, const KrylovBufs<float> &kb, const float *rhs, float *x,
                  double tol, int limit, int *count) {
-  return gmres_t<float>(c, ops, kb, rhs, x, tol, limit, true, false, count, nullptr);
+  return gmres_t<float>(c, ops, kb, rhs, x, tol, limit, true, false, count, nullptr, -1.);
 }
 
 }  // namespace eg
