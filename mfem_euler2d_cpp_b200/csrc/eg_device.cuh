@@ -199,37 +199,38 @@ __device__ bool cta_lu_solve(double *A, int lda, double *B, int ldb, int m, int 
   const int ncols = m + nb;
   for (int j = 0; j < m; ++j) {
     if (warp == 0) {
-      double best = -1.;
+      // largest magnitude, first row on ties, NaN never chosen: magnitudes
+      // compared as IEEE bit patterns (integer compares, warp reductions)
+      constexpr unsigned long long kAbs = 0x7fffffffffffffffull, kInf = 0x7ff0000000000000ull;
+      unsigned long long best = 0ull;
       int bi = m;
       for (int i = j + lane; i < m; i += 32) {
-        const double v = fabs(A[i + (size_t)j * lda]);
-        if (v > best) {
-          best = v;
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(A[i + (size_t)j * lda]) & kAbs;
+        if (bits <= kInf && (bi == m || bits > best)) {
+          best = bits;
           bi = i;
         }
       }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, off);
-        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
+      const unsigned hi = (unsigned)(best >> 32), lo = (unsigned)best;
+      const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+      const bool c1 = bi < m && hi == mhi;
+      const unsigned mlo = __reduce_max_sync(0xffffffffu, c1 ? lo : 0u);
+      bi = (int)__reduce_min_sync(0xffffffffu, c1 && lo == mlo ? (unsigned)bi : (unsigned)m);
       if (lane == 0) {
         // an all-NaN column leaves bi == m: report it as a zero pivot
         const double pv = bi < m ? A[bi + (size_t)j * lda] : 0.;
         piv[j] = bi < m ? bi : j;
         bcast[0] = pv;
-        inv_piv[j] = 1.0 / pv;
+        const double ip = 1.0 / pv;
+        bcast[1] = ip;
+        inv_piv[j] = ip;
       }
     }
     __syncthreads();
     const int p = piv[j];
     const double pv = bcast[0];
     if (!(fabs(pv) > 0.)) return false;
-    const double inv = 1.0 / pv;
+    const double inv = bcast[1];
     // multipliers of this lane's rows (virtual exchange of rows j and p)
     double lm[RMAX];
 #pragma unroll
