@@ -286,16 +286,20 @@ __global__ void __launch_bounds__(256) block_apply_kernel(const double *__restri
 }
 
 // The same apply with the block's part of x in registers (lane holds rows
-// lane + 32 r, r < R): sweep steps communicate through shuffles only, so the
-// loads of later factor columns, which do not depend on x, are issued ahead
-// of the arithmetic (unrolled column loops) instead of exposing one global
-// latency per step. The diagonal is applied as a product with its
-// reciprocal, formed off the dependency chain.
+// lane + 32 r, r < R): sweep steps communicate through shuffles only. Every
+// step reads one column of the factor; those reads do not depend on x, so
+// they are issued PD steps ahead into a register ring (fully unrolled sweeps,
+// static ring slots) and a step no longer waits out a memory latency. Column
+// and row indices are clamped into the block for the loads; only the
+// updates are predicated. The diagonal is applied as a product with its
+// reciprocal.
 template <int R>
 __global__ void __launch_bounds__(256) block_apply_reg_kernel(const double *__restrict__ blocks,
                                                               const int *__restrict__ piv, int nblocks,
                                                               int m, const double *__restrict__ b,
                                                               double *__restrict__ x) {
+  constexpr int S = 32 * R;                             // sweep steps (j >= m are no-ops)
+  constexpr int PD = R == 1 ? 16 : (R == 2 ? 8 : (R <= 4 ? 4 : (R <= 8 ? 2 : 1)));  // columns per chunk
   extern __shared__ double xs[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int blk = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -318,40 +322,71 @@ __global__ void __launch_bounds__(256) block_apply_reg_kernel(const double *__re
   double xr[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) xr[r] = lane + 32 * r < m ? v[lane + 32 * r] : 0.;
-  // forward: unit lower triangle
+  int rows[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) rows[r] = min(lane + 32 * r, m - 1);
+  auto load_col = [&](double (&dst)[R], int j) {
+    const double *col = lu + (size_t)min(max(j, 0), m - 1) * m;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[r] = col[rows[r]];
+  };
+  // columns are read in chunks of PD: the next chunk's loads are issued
+  // before the current chunk's steps (double buffer in registers)
+  double cur[PD][R], nxt[PD][R];
+  // forward: unit lower triangle, columns 0, 1, ...
+#pragma unroll
+  for (int d = 0; d < PD; ++d) load_col(cur[d], d);
 #pragma unroll
   for (int jb = 0; jb < R; ++jb) {
-#pragma unroll 8
-    for (int jl = 0; jl < 32; ++jl) {
-      const int j = 32 * jb + jl;
-      if (j < m) {
-        const double xj = __shfl_sync(0xffffffffu, xr[jb], jl);
-        const double *col = lu + (size_t)j * m;
+#pragma unroll 1
+    for (int cc = 0; cc < 32 / PD; ++cc) {
+      const int j0 = 32 * jb + PD * cc;
 #pragma unroll
-        for (int r = jb; r < R; ++r) {
+      for (int d = 0; d < PD; ++d) load_col(nxt[d], j0 + PD + d);
+#pragma unroll
+      for (int d = 0; d < PD; ++d) {
+        const int j = j0 + d;
+        const double xj = __shfl_sync(0xffffffffu, xr[jb], PD * cc + d);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
           const int i = lane + 32 * r;
-          if (i > j && i < m) xr[r] -= col[i] * xj;
+          xr[r] = (j < m && i > j && i < m) ? xr[r] - cur[d][r] * xj : xr[r];
         }
       }
+#pragma unroll
+      for (int d = 0; d < PD; ++d)
+#pragma unroll
+        for (int r = 0; r < R; ++r) cur[d][r] = nxt[d][r];
     }
   }
-  // backward: upper triangle with its diagonal
+  // backward: upper triangle with its diagonal, columns S-1, S-2, ...
+#pragma unroll
+  for (int d = 0; d < PD; ++d) load_col(cur[d], S - 1 - d);
 #pragma unroll
   for (int jb = R - 1; jb >= 0; --jb) {
-#pragma unroll 8
-    for (int jl = 31; jl >= 0; --jl) {
-      const int j = 32 * jb + jl;
-      if (j < m) {
-        const double *col = lu + (size_t)j * m;
-        const double rd = 1.0 / col[j];
-        const double xo = __shfl_sync(0xffffffffu, xr[jb], jl) * rd;
-        if (lane == jl) xr[jb] = xo;
+#pragma unroll 1
+    for (int cc = 32 / PD - 1; cc >= 0; --cc) {
+      const int jtop = 32 * jb + PD * cc + PD - 1;  // first (highest) column of the chunk
 #pragma unroll
-        for (int r = 0; r <= jb; ++r) {
+      for (int d = 0; d < PD; ++d) load_col(nxt[d], jtop - PD - d);
+#pragma unroll
+      for (int d = 0; d < PD; ++d) {
+        const int j = jtop - d;
+        const int jl = PD * cc + PD - 1 - d;  // j % 32
+        // u_jj sits in lane j % 32, register j / 32 (= jb) of this column
+        const double ujj = __shfl_sync(0xffffffffu, cur[d][jb], jl);
+        const double xo = __shfl_sync(0xffffffffu, xr[jb], jl) * (1.0 / ujj);
+        if (j < m && lane == jl) xr[jb] = xo;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
           const int i = lane + 32 * r;
-          if (i < j) xr[r] -= col[i] * xo;
+          xr[r] = (j < m && i < j) ? xr[r] - cur[d][r] * xo : xr[r];
         }
       }
+#pragma unroll
+      for (int d = 0; d < PD; ++d)
+#pragma unroll
+        for (int r = 0; r < R; ++r) cur[d][r] = nxt[d][r];
     }
   }
 #pragma unroll
