@@ -476,7 +476,9 @@ void launch_dg_jacobi(Ctx &c, const double *u, bool factor) {
 
 void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,
                         const double *b, double *x) {
-  const int warps = 8;
+  // 4 warps (blocks) per CTA: the register-resident sweeps use ~100
+  // registers, so smaller CTAs pack more warps per SM
+  const int warps = 4;
   const int grid = (nblocks + warps - 1) / warps;
   const size_t dyn = sizeof(double) * bs * warps;
   ProfScope ps(c, EG_K_PC_APPLY, 1);
