@@ -240,20 +240,30 @@ __device__ bool cta_lu_solve(double *A, int lda, double *B, int ldb, int m, int 
       if (i < m) v = (i == p ? A[j + (size_t)j * lda] : A[i + (size_t)j * lda]) * inv;
       lm[k] = v;
     }
-    for (int l = j + 1 + warp; l < ncols; l += nwarps) {
-      double *col = l < m ? A + (size_t)l * lda : B + (size_t)(l - m) * ldb;
-      const double top = col[p];   // value moving to row j
-      const double old_j = col[j]; // value moving to row p
+    // two of this warp's columns per iteration (the same columns per warp as
+    // one at a time): their reads overlap and share one warp sync
+    for (int l0 = j + 1 + warp; l0 < ncols; l0 += 2 * nwarps) {
+      const int l1 = l0 + nwarps;
+      const bool two = l1 < ncols;
+      double *c0 = l0 < m ? A + (size_t)l0 * lda : B + (size_t)(l0 - m) * ldb;
+      double *c1 = !two ? c0 : (l1 < m ? A + (size_t)l1 * lda : B + (size_t)(l1 - m) * ldb);
+      const double top0 = c0[p], old0 = c0[j];  // values moving to rows j and p
+      const double top1 = c1[p], old1 = c1[j];
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < RMAX; ++k) {
         const int i = j + 1 + lane + 32 * k;
         if (i < m) {
-          const double cur = (i == p) ? old_j : col[i];
-          col[i] = cur - lm[k] * top;
+          const double cur0 = (i == p) ? old0 : c0[i];
+          const double cur1 = (i == p) ? old1 : c1[i];
+          c0[i] = cur0 - lm[k] * top0;
+          if (two) c1[i] = cur1 - lm[k] * top1;
         }
       }
-      if (lane == 0) col[j] = top;
+      if (lane == 0) {
+        c0[j] = top0;
+        if (two) c1[j] = top1;
+      }
       __syncwarp();
     }
     __syncthreads();
