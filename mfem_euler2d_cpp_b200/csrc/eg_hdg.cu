@@ -193,207 +193,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Register-resident condensation for cells whose augmented system
-// [A | B | r] (m x (m + 4t + 1)) fits the register file of one CTA.
-// The system is staged in shared memory, then held in registers in a 2-D
-// block-cyclic layout over a TR x TC thread grid: thread (tr, tc) owns rows
-// tr + i*TR and columns tc + k*TC. Each elimination step broadcasts the
-// pivot column and the new pivot row through double-buffered shared
-// memory (two barriers per step; every warp finds the pivot itself), then
-// every thread updates its block of the trailing matrix with FMAs on
-// registers. Pivoting is partial by rows with the first maximum winning,
-// multipliers are a_ij * (1/pivot), and the upper solve divides by the
-// pivot, as in MFEM LUFactors::Factor/Solve. Back substitution runs on the
-// right-hand-side columns in registers (one barrier per step).
-template <int Q, int TR, int TC>
-struct RegCfg {
-  static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, NC = M + NR;
-  static constexpr int RP = (M + TR - 1) / TR, CP = (NC + TC - 1) / TC;
-  static constexpr int THREADS = TR * TC;
-};
-
-template <int Q, int TR, int TC, int MINB>
-__global__ void __launch_bounds__(TR *TC, MINB)
-    condense_reg_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
-                        const double *__restrict__ r, double *XY, double *Cb, double *sf_out,
-                        double *contrib, double *panels, int *err) {
-  using C = RegCfg<Q, TR, TC>;
-  constexpr int M = C::M, NC = C::NC, RP = C::RP, CP = C::CP;
-  __shared__ CondenseShared<Q> sh;
-  __shared__ double colbuf[2][M], rowbuf[2][NC], rowold[2][NC];
-  extern __shared__ double dyn[];  // augmented system, column-major M x NC
-  const int tr = threadIdx.x % TR, tc = threadIdx.x / TR;
-  const int lane = threadIdx.x & 31;
-  load_tables<Q>(sh.st, tab);
-  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
-    __syncthreads();
-    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, dyn, dyn + (size_t)M * M, e);
-    __syncthreads();
-    double a[RP][CP];
-#pragma unroll
-    for (int i = 0; i < RP; ++i) {
-      const int row = tr + i * TR;
-#pragma unroll
-      for (int k = 0; k < CP; ++k) {
-        const int col = tc + k * TC;
-        a[i][k] = (row < M && col < NC) ? dyn[row + (size_t)col * M] : 0.;
-      }
-    }
-    bool singular = false;
-    for (int j = 0; j < M; ++j) {
-      const int buf = j & 1;
-      const int jk = j / TC, ji = j / TR;
-      if (tc == j % TC) {
-#pragma unroll
-        for (int i = 0; i < RP; ++i) {
-          const int row = tr + i * TR;
-          if (row >= j && row < M) {
-            double v = 0.;
-#pragma unroll
-            for (int k = 0; k < CP; ++k)
-              if (k == jk) v = a[i][k];
-            colbuf[buf][row] = v;
-          }
-        }
-      }
-      __syncthreads();
-      double best = -1.;
-      int bi = M;
-      for (int i = j + lane; i < M; i += 32) {
-        const double v = fabs(colbuf[buf][i]);
-        if (v > best) {
-          best = v;
-          bi = i;
-        }
-      }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      const int p = bi < M ? bi : j;  // an all-NaN column leaves bi == M
-      const double pv = bi < M ? colbuf[buf][p] : 0.;
-      if (!(fabs(pv) > 0.)) {
-        singular = true;
-        break;
-      }
-      const double inv = 1.0 / pv;
-      const int pi = p / TR;
-      if (tr == j % TR || tr == p % TR) {
-#pragma unroll
-        for (int k = 0; k < CP; ++k) {
-          const int col = tc + k * TC;
-          if (col < NC) {
-            double vj = 0., vp = 0.;
-#pragma unroll
-            for (int i = 0; i < RP; ++i) {
-              if (i == ji) vj = a[i][k];
-              if (i == pi) vp = a[i][k];
-            }
-            if (tr == j % TR) rowold[buf][col] = vj;
-            if (tr == p % TR) rowbuf[buf][col] = vp;
-          }
-        }
-      }
-      __syncthreads();
-      if (p != j && (tr == j % TR || tr == p % TR)) {
-#pragma unroll
-        for (int k = 0; k < CP; ++k) {
-          const int col = tc + k * TC;
-          if (col < NC) {
-#pragma unroll
-            for (int i = 0; i < RP; ++i) {
-              if (tr == j % TR && i == ji) a[i][k] = rowbuf[buf][col];
-              if (tr == p % TR && i == pi) a[i][k] = rowold[buf][col];
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < RP; ++i) {
-        const int row = tr + i * TR;
-        if (row > j && row < M) {
-          const double l = (row == p ? colbuf[buf][j] : colbuf[buf][row]) * inv;
-#pragma unroll
-          for (int k = 0; k < CP; ++k) {
-            const int col = tc + k * TC;
-            if (col > j && col < NC) {
-              a[i][k] -= l * rowbuf[buf][col];
-            } else if (col == j) {
-              a[i][k] = l;
-            }
-          }
-        }
-      }
-    }
-    if (singular) {
-      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
-      continue;
-    }
-    // U to shared memory for the back substitution
-#pragma unroll
-    for (int i = 0; i < RP; ++i) {
-      const int row = tr + i * TR;
-#pragma unroll
-      for (int k = 0; k < CP; ++k) {
-        const int col = tc + k * TC;
-        if (row < M && col < M) dyn[row + (size_t)col * M] = a[i][k];
-      }
-    }
-    __syncthreads();
-    for (int j = M - 1; j >= 0; --j) {
-      const int buf = j & 1;
-      const double ujj = dyn[j + (size_t)j * M];
-      if (tr == j % TR) {
-        const int ji = j / TR;
-#pragma unroll
-        for (int i = 0; i < RP; ++i) {
-          if (i == ji) {
-#pragma unroll
-            for (int k = 0; k < CP; ++k) {
-              const int col = tc + k * TC;
-              if (col >= M && col < NC) {
-                const double x = a[i][k] / ujj;
-                a[i][k] = x;
-                rowbuf[buf][col] = x;
-              }
-            }
-          }
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < RP; ++i) {
-        const int row = tr + i * TR;
-        if (row < j) {
-          const double uij = dyn[row + (size_t)j * M];
-#pragma unroll
-          for (int k = 0; k < CP; ++k) {
-            const int col = tc + k * TC;
-            if (col >= M && col < NC) a[i][k] -= uij * rowbuf[buf][col];
-          }
-        }
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < RP; ++i) {
-      const int row = tr + i * TR;
-#pragma unroll
-      for (int k = 0; k < CP; ++k) {
-        const int col = tc + k * TC;
-        if (row < M && col >= M && col < NC) dyn[row + (size_t)col * M] = a[i][k];
-      }
-    }
-    __syncthreads();
-    condense_epilogue<Q>(sh, dyn + (size_t)M * M, true, XY, contrib, panels, e);
-  }
-}
-
 // ------------------------------------------- tensor-core Gauss-Jordan
 // D = C + A B on the FP64 tensor pipe: m8n8k4, A row-major 8x4 (one element
 // per lane: row lane/4, column lane%4), B column-major 4x8 (row lane%4,
@@ -1280,18 +1079,6 @@ static int sm_count_hdg() {
 }
 
 static int condense_grid(Ctx &c) { return std::min(c.n, sm_count_hdg() * 4); }
-
-template <int Q, int TR, int TC, int MINB>
-static void launch_condense_reg(Ctx &c, const double *u, const double *r) {
-  using C = RegCfg<Q, TR, TC>;
-  constexpr size_t dyn = sizeof(double) * (size_t)C::M * C::NC;
-  auto kern = condense_reg_kernel<Q, TR, TC, MINB>;
-  if (dyn > 48 * 1024)
-    EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-  const int grid = std::min(c.n, sm_count_hdg() * MINB);
-  kern<<<grid, C::THREADS, dyn, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, r,
-                                            c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
-}
 
 template <int Q, int WR, int WC, int MINB>
 static void launch_condense_gj(Ctx &c, const double *u, const double *r) {
