@@ -110,3 +110,22 @@ def test_pc_apply_inverts_blocks(unit):
         b = np.sin(0.7 * np.arange(ctx.nl))
         want = np.linalg.solve(blocks, b.reshape(ctx.nf, t, 1)).ravel()
         assert rel_err(ctx.pc_apply(b), want) < 1e-11
+
+
+def test_hdg_jacobi_inverses_download(unit):
+    """The factored Schur block-Jacobi slot holds the explicit inverses of the
+    assembled blocks (both downloaded column-major): S_f Inv_f = I."""
+    f = unit
+    ctx, _ = _ctx(f, capi.FORM_HDG)
+    with ctx:
+        ctx.upload("R", f["r"])
+        ctx.condense()
+        t = ctx.t
+        ctx.pc_factor(False)
+        s = ctx.download("PC_BLOCKS").reshape(ctx.nf, t, t).transpose(0, 2, 1)
+        ctx.pc_factor(True)
+        inv = ctx.download("PC_BLOCKS").reshape(ctx.nf, t, t).transpose(0, 2, 1)
+        prod = np.einsum("fij,fjk->fik", s, inv)
+        eye = np.broadcast_to(np.eye(t), prod.shape)
+        scale = np.abs(s).max(axis=(1, 2)) * np.abs(inv).max(axis=(1, 2))
+        assert np.max(np.abs(prod - eye).max(axis=(1, 2)) / scale) < 1e-12
