@@ -112,6 +112,28 @@ def test_pc_apply_inverts_blocks(unit):
         assert rel_err(ctx.pc_apply(b), want) < 1e-11
 
 
+@pytest.mark.parametrize("nx,ny,k", [(7, 5, 0), (9, 8, 2), (11, 7, 4), (7, 4, 5), (5, 3, 8)])
+def test_hdg_pc_apply_matches_downloaded_inverses(nx, ny, k):
+    """The Schur block-Jacobi apply multiplies each face's explicit inverse by
+    that face's slice of b; the face counts leave the last group of faces a
+    CTA stages partly filled."""
+    d = capi.simple_wave_desc(nx, ny, k, 30.0)
+    with capi.Context(d, capi.default_opts(form=capi.FORM_HDG)) as ctx:
+        ctx.initial()
+        u = ctx.download("U")
+        ctx.freeze(1e-3, check_admissible=True)
+        ctx.upload("OLD", u)
+        ctx.set_dt(1e-3)
+        ctx.residual()
+        ctx.condense()
+        ctx.pc_factor(True)
+        t = ctx.t
+        inv = ctx.download("PC_BLOCKS").reshape(ctx.nf, t, t).transpose(0, 2, 1)
+        b = np.cos(0.37 * np.arange(ctx.nl)) + 0.1
+        want = np.einsum("fij,fj->fi", inv, b.reshape(ctx.nf, t)).ravel()
+        assert rel_err(ctx.pc_apply(b), want) < 1e-13
+
+
 def test_hdg_jacobi_inverses_download(unit):
     """The factored Schur block-Jacobi slot holds the explicit inverses of the
     assembled blocks (both downloaded column-major): S_f Inv_f = I."""
