@@ -65,7 +65,14 @@ enum eg_status {
 
 enum eg_form { EG_FORM_DG = 0, EG_FORM_HDG = 1 };
 enum eg_precond { EG_PC_BLOCK_JACOBI = 0, EG_PC_BLOCK_ILU0 = 1 };
-enum eg_assembly { EG_ASSEMBLY_PARTIAL = 0, EG_ASSEMBLY_FULL = 1 };
+/* Options::assembly (src/options.cpp:51-53, 130-146):
+ *  PARTIAL  matrix-free operators (DG: PartialDGOperator; HDG: the Schur action from C and X);
+ *  ELEMENT  element-assembled operators applied matrix-free (DG: the cell and face-coupling
+ *           blocks of the Jacobian; HDG: the per-cell Schur entries C X, src/condensation.cpp:143-146);
+ *  FULL     GMRES on the assembled block-sparse matrix (ElementOperator::Assemble,
+ *           src/operators.cpp:180-238), the final residual from the element operator
+ *           (src/linear.cpp:242-246). */
+enum eg_assembly { EG_ASSEMBLY_PARTIAL = 0, EG_ASSEMBLY_FULL = 1, EG_ASSEMBLY_ELEMENT = 2 };
 enum eg_precision {
   EG_PRECISION_FP64 = 0,  /* everything FP64 (parity path) */
   EG_PRECISION_MIXED = 1  /* FP32 preconditioner + FP32 inner Schur GMRES in FP64 refinement */

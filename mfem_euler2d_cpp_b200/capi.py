@@ -35,6 +35,7 @@ STATUS_NAMES = {
 FORM_DG, FORM_HDG = 0, 1
 PC_JACOBI, PC_ILU0 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+ASSEMBLY_PARTIAL, ASSEMBLY_FULL, ASSEMBLY_ELEMENT = 0, 1, 2
 SLOT = dict(U=0, OLD=1, R=2, DU=3, RHS=4, LAMBDA=5, D=6, X=7, Y=8, PC_BLOCKS=9, HLL_A=10, HLL_B=11)
 
 

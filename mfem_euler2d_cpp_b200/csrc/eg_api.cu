@@ -127,7 +127,7 @@ void Ctx::ensure_hdg() {
   Cb = alloc_n<double>((size_t)n * 4 * q * 16);
   sf = alloc_n<double>((size_t)n * 4 * q);
   contrib = alloc_n<double>((size_t)n * 4 * t);
-  panels = alloc_n<double>((size_t)n * (schur_panels_full(q) ? 16 : 4) * t * t);
+  panels = alloc_n<double>((size_t)n * geo.npan * t * t);
   rhs = alloc_n<double>(nl);
   lam = alloc_n<double>(nl);
   tmp_trace = alloc_n<double>(nl);
@@ -168,7 +168,14 @@ struct DgOps : LinearOps {
     mtab = c.mtab_dg;
     period = c.m;
   }
-  void apply(Ctx &c, const double *x, double *y) override { launch_dg_apply(c, c.u, x, y); }
+  // partial assembly: the Jacobian from the state inside every action;
+  // element/full: the assembled cell and face-coupling blocks
+  void apply(Ctx &c, const double *x, double *y) override {
+    if (c.opts.assembly == EG_ASSEMBLY_PARTIAL)
+      launch_dg_apply(c, c.u, x, y);
+    else
+      launch_assembled_apply(c, EG_FORM_DG, x, y);
+  }
   void precondition(Ctx &c, const double *b, double *x) override {
     if (c.opts.precond == EG_PC_BLOCK_ILU0)
       launch_ilu_apply(c, EG_FORM_DG, b, x);
@@ -184,7 +191,13 @@ struct HdgOps : LinearOps {
     // the block-Jacobi and Schur kernels honour Ctx::skip; the ILU sweeps do not
     group = c.opts.precond == EG_PC_BLOCK_ILU0 ? 1 : kArnoldiGroup;
   }
-  void apply(Ctx &c, const double *x, double *y) override { launch_schur_apply(c, x, y); }
+  // partial/element: the per-cell Schur action; full: the assembled matrix
+  void apply(Ctx &c, const double *x, double *y) override {
+    if (c.opts.assembly == EG_ASSEMBLY_FULL)
+      launch_assembled_apply(c, EG_FORM_HDG, x, y);
+    else
+      launch_schur_apply(c, x, y);
+  }
   void precondition(Ctx &c, const double *b, double *x) override {
     if (c.opts.precond == EG_PC_BLOCK_ILU0)
       launch_ilu_apply(c, EG_FORM_HDG, b, x);
@@ -225,7 +238,15 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
     if (eq) launch_fill(c, ops.N, 0., eq);
     return;
   }
+  // assembled operator: ElementOperator::Assemble for full assembly and the
+  // element-assembled DG Jacobian (src/linear.cpp:186-190, stepper.cpp:139-140);
+  // the element-assembled Schur entries come with the condensation
+  const bool assembled = form == EG_FORM_DG ? c.opts.assembly != EG_ASSEMBLY_PARTIAL
+                                            : c.opts.assembly == EG_ASSEMBLY_FULL;
   double t0 = now_s();
+  if (refresh && assembled) assemble_blocks(c, form);
+  out.assembly = now_s() - t0;
+  t0 = now_s();
   if (refresh) {
     pc_factor(c, form, true);
   }
@@ -251,7 +272,19 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
   c.check_device_error();
   out.solve = now_s() - t0;
   out.count = count;
-  if (eq) launch_axpby(c, ops.N, -1., c.kres, 0., c.kres, eq);
+  if (c.opts.assembly == EG_ASSEMBLY_FULL) {
+    // GMRES ran on the assembled matrix: the residual comes from the
+    // element operator's own action (src/linear.cpp:242-246)
+    double *dst = eq ? eq : c.kres;
+    if (form == EG_FORM_DG)
+      launch_dg_apply(c, c.u, x, c.kw);
+    else
+      launch_schur_apply(c, x, c.kw);
+    launch_axpby(c, ops.N, 1., c.kw, -1., rhs, dst);
+    res = wnorm(c, dst, ops.N, ops.mtab, ops.period);
+  } else if (eq) {
+    launch_axpby(c, ops.N, -1., c.kres, 0., c.kres, eq);
+  }
   out.residual = res / rhs_norm;
   if (!(std::isfinite(out.residual) && out.residual <= std::max(10 * tol, 1e-12)))
     fail(EG_ERR_LINEAR_RESIDUAL, "True inverse-mass weighted linear residual too large");
@@ -378,7 +411,8 @@ void newton_update(Ctx &c, double residual_norm, double old_norm, eg_update_stat
 // [mass][ew]; dual-norm metric tables), uploaded in stream order.
 void upload_desc(Ctx &c, const eg_desc &d) {
   c.desc = d;
-  c.geo = Geo{d.nx, d.ny, c.n, c.nf, d.hx, d.hy, d.area, c.geo.dt, d.gamma, d.gamma - 1., d.safety};
+  c.geo = Geo{d.nx, d.ny, c.n, c.nf, d.hx, d.hy, d.area, c.geo.dt, d.gamma, d.gamma - 1., d.safety,
+              schur_panels_full(c.q) || c.opts.assembly != EG_ASSEMBLY_PARTIAL ? 16 : 4};
   const int q = c.q, p = c.p;
   std::vector<double> tab(tab_size(q));
   for (int i = 0; i < p; ++i) {
@@ -500,6 +534,10 @@ static void validate_opts(const eg_opts &o) {
   if (!(o.linear_tol > 0)) eg::fail(EG_ERR_INVALID, "linear tolerance must be positive");
   if (o.precision != EG_PRECISION_FP64 && o.precision != EG_PRECISION_MIXED)
     eg::fail(EG_ERR_INVALID, "Invalid precision");
+  if (o.assembly != EG_ASSEMBLY_PARTIAL && o.assembly != EG_ASSEMBLY_ELEMENT && o.assembly != EG_ASSEMBLY_FULL)
+    eg::fail(EG_ERR_INVALID, "Invalid assembly");
+  if (o.precision == EG_PRECISION_MIXED && o.assembly == EG_ASSEMBLY_FULL)
+    eg::fail(EG_ERR_INVALID, "mixed precision requires partial or element assembly");
 }
 
 int eg_create(const eg_desc *d, const eg_opts *o, eg_ctx **out) {
@@ -595,6 +633,8 @@ int eg_set_opts(eg_ctx *ctx, const eg_opts *o) {
   return guard(ctx, [&] {
     validate_opts(*o);
     if (o->restart > ctx->c.kR && ctx->c.V) eg::fail(EG_ERR_INVALID, "restart cannot grow after first solve");
+    if (o->assembly != ctx->c.opts.assembly)
+      eg::fail(EG_ERR_INVALID, "assembly is fixed when the context is created");
     ctx->c.opts = *o;
     if (o->form == EG_FORM_HDG) ctx->c.ensure_hdg();
   });

@@ -12,6 +12,7 @@ namespace eg {
 struct Geo {
   int nx, ny, n, nf;
   double hx, hy, area, dt, gamma, gm1, safety;
+  int npan;  // Schur panels C_s X_o stored per cell: the 4 diagonal ones or all 16
 };
 
 // Frozen per-face-point HLL data (src/problem.cpp:357-374), SoA of nf*q.

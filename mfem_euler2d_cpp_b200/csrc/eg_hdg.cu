@@ -118,7 +118,7 @@ __device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen
 // panels C_s X_s (src/operators.cpp:7-26, 295-301).
 template <int Q>
 __device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, bool copy_out, double *XY,
-                                  double *contrib, double *panels, int e) {
+                                  double *contrib, double *panels, int npan, int e) {
   constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
   const STab<Q> &st = sh.st;
   if (copy_out) {
@@ -143,10 +143,10 @@ __device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, 
   }
   if (panels) {
     // the 4 diagonal panels, or all 16 ([s][o]) where the Schur action uses them
-    constexpr int NPAN = schur_panels_full(Q) ? 16 : 4;
-    for (int o = threadIdx.x; o < NPAN * T * T; o += blockDim.x) {
+    const bool all16 = npan == 16;
+    for (int o = threadIdx.x; o < npan * T * T; o += blockDim.x) {
       const int pan = o / (T * T), rem = o % (T * T);
-      const int s = NPAN == 16 ? pan >> 2 : pan, so = NPAN == 16 ? pan & 3 : pan;
+      const int s = all16 ? pan >> 2 : pan, so = all16 ? pan & 3 : pan;
       const int row = rem % T, cc = rem / T;
       const int jj = row >> 2, c = row & 3;
       const double *xc = R + (size_t)(so * T + cc) * M;
@@ -161,7 +161,7 @@ __device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, 
       double res = 0.;
 #pragma unroll
       for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
-      panels[(size_t)e * NPAN * T * T + o] = res;
+      panels[(size_t)e * npan * T * T + o] = res;
     }
   }
 }
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256)
       if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
       continue;
     }
-    condense_epilogue<Q>(sh, R, MODE == 0, XY, contrib, panels, e);
+    condense_epilogue<Q>(sh, R, MODE == 0, XY, contrib, panels, g.npan, e);
   }
 }
 
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
       }
     }
     __syncthreads();
-    condense_epilogue<Q>(sh, R, true, XY, contrib, panels, e);
+    condense_epilogue<Q>(sh, R, true, XY, contrib, panels, g.npan, e);
   }
 }
 
@@ -752,7 +752,7 @@ __global__ void __launch_bounds__(256, GjgCfg<Q>::MINB)
       R[o] = W[(size_t)(M + c) * M + piv[j]];
     }
     __syncthreads();
-    condense_epilogue<Q>(sh, R, false, XY, contrib, panels, e);
+    condense_epilogue<Q>(sh, R, false, XY, contrib, panels, g.npan, e);
   }
 }
 
@@ -810,11 +810,13 @@ __global__ void __launch_bounds__(128)
 }
 
 // Schur action from the 16 panels of a cell (degrees with
-// schur_panels_full): contrib[e][s] = sum_o (C_s X_o) v_o, the same product as
-// the C restriction of X v (src/operators.cpp:166-178) with the C X panels
-// formed once per condensation, so that each apply streams 16 t^2 doubles per
-// cell instead of m x 4t. One thread per output (s, row); consecutive rows
-// read consecutive panel entries.
+// schur_panels_full, and every degree with element or full assembly, where the
+// panels are the element entries C X of src/condensation.cpp:143-146):
+// contrib[e][s] = sum_o (C_s X_o) v_o, the same product as the C restriction
+// of X v (src/operators.cpp:166-178) with the C X panels formed once per
+// condensation, so that each apply streams 16 t^2 doubles per cell instead of
+// m x 4t. One thread per output (s, row); consecutive rows read consecutive
+// panel entries.
 template <int Q>
 __global__ void __launch_bounds__(((16 * Q + 31) / 32) * 32)
     panel_gemv_kernel(Geo g, const double *__restrict__ panels, const double *__restrict__ v,
@@ -890,7 +892,7 @@ __global__ void __launch_bounds__(256)
 // coalesced batched GEMV instead of two dependent triangular sweeps.
 template <int T>
 __global__ void __launch_bounds__(64)
-    schur_jacobi_kernel(int nx, int ny, int nf, const double *__restrict__ D,
+    schur_jacobi_kernel(int nx, int ny, int nf, int npan, const double *__restrict__ D,
                         const double *__restrict__ panels, double *blocks, int *pivots, bool factor,
                         int *err) {
   __shared__ double S[T * T], Inv[T * T];
@@ -901,11 +903,10 @@ __global__ void __launch_bounds__(64)
     __syncthreads();
     const int L = f >> 1, ls = (f & 1) ? 3 : 1;
     const int R = neighbour(L, ls, nx, ny), rs = ls - 1;
-    // diagonal panels C_s X_s of the two cells (16 panels per cell where the
-    // Schur action keeps them all)
-    constexpr bool kFull = schur_panels_full(T / 4);
-    const double *pl = panels + (kFull ? (size_t)L * 16 + ls * 5 : (size_t)L * 4 + ls) * T * T;
-    const double *pr = panels + (kFull ? (size_t)R * 16 + rs * 5 : (size_t)R * 4 + rs) * T * T;
+    // diagonal panels C_s X_s of the two cells (panel s*5 of 16 where all are kept)
+    const bool all16 = npan == 16;
+    const double *pl = panels + (all16 ? (size_t)L * 16 + ls * 5 : (size_t)L * 4 + ls) * T * T;
+    const double *pr = panels + (all16 ? (size_t)R * 16 + rs * 5 : (size_t)R * 4 + rs) * T * T;
     for (int o = threadIdx.x; o < T * T; o += blockDim.x) {
       const int row = o % T, col = o / T;
       const double d = row == col ? D[(size_t)f * T + row] : 0.;
@@ -935,7 +936,7 @@ __global__ void __launch_bounds__(64)
 // `pivots` receives the pivot row of every step. Blocks are stored row-major.
 template <int T>
 __global__ void __launch_bounds__(128)
-    schur_jacobi_warp_kernel(int nx, int ny, int nf, const double *__restrict__ D,
+    schur_jacobi_warp_kernel(int nx, int ny, int nf, int npan, const double *__restrict__ D,
                              const double *__restrict__ panels, double *blocks, int *pivots, bool factor,
                              int *err) {
   static_assert(T <= 32, "one row per lane");
@@ -945,11 +946,10 @@ __global__ void __launch_bounds__(128)
   for (int f = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); f < nf; f += nwarps) {
     const int L = f >> 1, ls = (f & 1) ? 3 : 1;
     const int R = neighbour(L, ls, nx, ny), rs = ls - 1;
-    // diagonal panels C_s X_s of the two cells (16 panels per cell where the
-    // Schur action keeps them all)
-    constexpr bool kFull = schur_panels_full(T / 4);
-    const double *pl = panels + (kFull ? (size_t)L * 16 + ls * 5 : (size_t)L * 4 + ls) * T * T;
-    const double *pr = panels + (kFull ? (size_t)R * 16 + rs * 5 : (size_t)R * 4 + rs) * T * T;
+    // diagonal panels C_s X_s of the two cells (panel s*5 of 16 where all are kept)
+    const bool all16 = npan == 16;
+    const double *pl = panels + (all16 ? (size_t)L * 16 + ls * 5 : (size_t)L * 4 + ls) * T * T;
+    const double *pr = panels + (all16 ? (size_t)R * 16 + rs * 5 : (size_t)R * 4 + rs) * T * T;
     const bool row_ok = lane < T;
     const double d = row_ok ? D[(size_t)f * T + lane] : 0.;
     double sr[T], xr[T];
@@ -1150,14 +1150,14 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
 void launch_schur_apply(Ctx &c, const double *v, double *y) {
   ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
   const int grid = std::min(c.n, sm_count_hdg() * 16);
-  if (schur_panels_full(c.q)) {
+  if (c.geo.npan == 16) {
     switch (c.q) {
 #define EG_PG(QQ)                                                                                          \
   case QQ:                                                                                                 \
     panel_gemv_kernel<QQ><<<grid, ((16 * QQ + 31) / 32) * 32, 0, c.stream>>>(c.geo, c.panels, v, c.contrib, \
                                                                             c.skip);                       \
     break;
-      EG_PG(5) EG_PG(6) EG_PG(7) EG_PG(8) EG_PG(9)
+      EG_PG(1) EG_PG(2) EG_PG(3) EG_PG(4) EG_PG(5) EG_PG(6) EG_PG(7) EG_PG(8) EG_PG(9)
 #undef EG_PG
       default:
         fail(EG_ERR_INVALID, "unsupported degree");
@@ -1221,13 +1221,13 @@ void launch_schur_jacobi(Ctx &c, bool factor) {
   switch (c.t) {
 #define EG_SJW(TT)                                                                                     \
   case TT:                                                                                             \
-    schur_jacobi_warp_kernel<TT><<<wgrid, 128, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.D, c.panels, \
+    schur_jacobi_warp_kernel<TT><<<wgrid, 128, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.geo.npan, c.D, c.panels, \
                                                               c.pc_hdg, c.piv_hdg, factor, c.derr);      \
     break;
     EG_SJW(4) EG_SJW(8) EG_SJW(12) EG_SJW(16) EG_SJW(20) EG_SJW(24) EG_SJW(28) EG_SJW(32)
 #undef EG_SJW
     case 36:
-      schur_jacobi_kernel<36><<<grid, 64, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.D, c.panels, c.pc_hdg,
+      schur_jacobi_kernel<36><<<grid, 64, 0, c.stream>>>(c.desc.nx, c.desc.ny, c.nf, c.geo.npan, c.D, c.panels, c.pc_hdg,
                                                          c.piv_hdg, factor, c.derr);
       break;
     default:

@@ -739,7 +739,7 @@ void build_plan(Ctx &c, int form) {
   P.w = c.alloc_n<double>((size_t)P.rows * P.B);
   // the condensation keeps all 16 panels per cell where the Schur action
   // streams them (same layout and arithmetic); otherwise the fill forms them
-  if (hdg && !schur_panels_full(c.q)) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
+  if (hdg && c.geo.npan != 16) P.panels16 = c.alloc_n<double>((size_t)c.n * 16 * BB);
   if (!P.staged) P.work = c.alloc_n<double>((size_t)G * 3 * BB);
   P.progress = c.alloc_n<unsigned long long>(G);
   EG_CUDA(cudaMemsetAsync(P.progress, 0, sizeof(unsigned long long) * G, c.stream));
@@ -837,6 +837,54 @@ void factor_dispatch(Ctx &c, IluPlan &P) {
   }
 }
 
+// Numeric blocks of the plan's structure into dst (nnzb x B^2, column-major).
+void fill_blocks(Ctx &c, int form, IluPlan &P, double *dst) {
+  const bool hdg = form == EG_FORM_HDG;
+  const int sms = sm_count_ilu();
+  if (hdg) {
+    const double *pan16 = c.geo.npan == 16 ? c.panels : P.panels16;
+    if (c.geo.npan != 16) {
+      const long long np = (long long)c.n * 16 * c.t * c.t;
+      const int grid = (int)std::min<long long>((np + 255) / 256, (long long)sms * 16);
+      EG_DISPATCH_Q(c.q, (ilu_panels_kernel<Q><<<grid, 256, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb, P.panels16)));
+      EG_CUDA(cudaGetLastError());
+    }
+    const long long ne = (long long)P.nnzb * c.t * c.t;
+    const int g2 = (int)std::min<long long>((ne + 255) / 256, (long long)sms * 16);
+    ilu_fill_hdg_kernel<<<g2, 256, 0, c.stream>>>(P.nnzb, c.t, P.erow, P.col, P.fill_ptr, P.fill_src, c.D,
+                                                  pan16, dst);
+  } else {
+    const int grid = std::min(P.nnzb, sms * 8);
+    EG_DISPATCH_Q(c.q, (ilu_fill_dg_kernel<Q><<<grid, 256, 0, c.stream>>>(
+                           c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, c.u, P.nnzb, P.erow, P.col,
+                           P.fill_ptr, P.fill_src, dst)));
+  }
+  EG_CUDA(cudaGetLastError());
+}
+
+// y = A x for an assembled block-sparse operator: one thread per scalar row;
+// blocks are column-major, so consecutive rows of a block read adjacent
+// entries, and block columns come in increasing order (the column order of
+// the assembled CSR rows, src/operators.cpp:180-238).
+__global__ void __launch_bounds__(256)
+    bsr_spmv_kernel(int rows, int B, const int *__restrict__ rowp, const int *__restrict__ col,
+                    const double *__restrict__ data, const double *__restrict__ x, double *__restrict__ y,
+                    const int *__restrict__ skip) {
+  if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (long long)rows * B) return;
+  const int i = (int)(id / B), r = (int)(id % B);
+  const size_t BB = (size_t)B * B;
+  double acc = 0.;
+  for (int k = rowp[i]; k < rowp[i + 1]; ++k) {
+    const double *a = data + (size_t)k * BB + r;
+    const double *xv = x + (size_t)col[k] * B;
+#pragma unroll 4
+    for (int j = 0; j < B; ++j) acc += a[(size_t)j * B] * xv[j];
+  }
+  y[id] = acc;
+}
+
 }  // namespace
 
 void ilu_refresh(Ctx &c, int form, bool factor) {
@@ -846,27 +894,36 @@ void ilu_refresh(Ctx &c, int form, bool factor) {
   if (hdg && !c.condensed) fail(EG_ERR_INVALID, "Schur preconditioner requires a condensation");
   ProfScope ps(c, hdg ? EG_K_SCHUR_JACOBI : EG_K_DG_JACOBI, factor ? 3 : 2);
   EG_CUDA(cudaMemsetAsync(P.abort, 0, sizeof(int), c.stream));
-  const int sms = sm_count_ilu();
-  if (hdg) {
-    const double *pan16 = schur_panels_full(c.q) ? c.panels : P.panels16;
-    if (!schur_panels_full(c.q)) {
-      const long long np = (long long)c.n * 16 * c.t * c.t;
-      const int grid = (int)std::min<long long>((np + 255) / 256, (long long)sms * 16);
-      EG_DISPATCH_Q(c.q, (ilu_panels_kernel<Q><<<grid, 256, 0, c.stream>>>(c.geo, c.tab, c.XY, c.Cb, P.panels16)));
-      EG_CUDA(cudaGetLastError());
-    }
-    const long long ne = (long long)P.nnzb * c.t * c.t;
-    const int g2 = (int)std::min<long long>((ne + 255) / 256, (long long)sms * 16);
-    ilu_fill_hdg_kernel<<<g2, 256, 0, c.stream>>>(P.nnzb, c.t, P.erow, P.col, P.fill_ptr, P.fill_src, c.D,
-                                                  pan16, P.data);
-  } else {
-    const int grid = std::min(P.nnzb, sms * 8);
-    EG_DISPATCH_Q(c.q, (ilu_fill_dg_kernel<Q><<<grid, 256, 0, c.stream>>>(
-                           c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, c.u, P.nnzb, P.erow, P.col,
-                           P.fill_ptr, P.fill_src, P.data)));
-  }
-  EG_CUDA(cudaGetLastError());
+  fill_blocks(c, form, P, P.data);
   if (factor) factor_dispatch(c, P);
+}
+
+// ElementOperator::Assemble (src/operators.cpp:180-238) for full assembly and
+// the element-assembled DG Jacobian (Problem::DG, src/problem.cpp:552-588):
+// the blocks the ILU(0) fill sums (FillBlocks), left unfactored.
+void assemble_blocks(Ctx &c, int form) {
+  const bool hdg = form == EG_FORM_HDG;
+  if (hdg && !c.condensed) fail(EG_ERR_INVALID, "assembled Schur operator requires a condensation");
+  build_plan(c, form);
+  IluPlan &P = c.ilu[form];
+  ProfScope ps(c, EG_K_VECTOR, 2);
+  if (c.opts.precond == EG_PC_BLOCK_ILU0) {
+    if (!P.asm_own) P.asm_own = c.alloc_n<double>((size_t)P.nnzb * P.B * P.B);
+    P.asmd = P.asm_own;
+  } else {
+    P.asmd = P.data;  // unused by block Jacobi
+  }
+  fill_blocks(c, form, P, P.asmd);
+}
+
+void launch_assembled_apply(Ctx &c, int form, const double *x, double *y) {
+  IluPlan &P = c.ilu[form];
+  if (!P.built || !P.asmd) fail(EG_ERR_INVALID, "no assembled operator");
+  ProfScope ps(c, form == EG_FORM_HDG ? EG_K_SCHUR_APPLY : EG_K_DG_APPLY, 2);
+  const long long total = (long long)P.rows * P.B;
+  bsr_spmv_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c.stream>>>(P.rows, P.B, P.row, P.col, P.asmd, x,
+                                                                         y, c.skip);
+  EG_CUDA(cudaGetLastError());
 }
 
 void launch_ilu_apply(Ctx &c, int form, const double *b, double *x) {

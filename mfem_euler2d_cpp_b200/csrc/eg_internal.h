@@ -129,6 +129,9 @@ struct IluPlan {
   int *fill_ptr = nullptr, *fill_src = nullptr;  // per entry: fill contributions
   double *data = nullptr, *dinv = nullptr, *w = nullptr;
   double *panels16 = nullptr;                    // HDG: 16 panels C_s X_o per cell
+  // element/full assembly: the operator's blocks, unfactored (`data` itself
+  // while the preconditioner is block Jacobi, a separate array under ILU(0))
+  double *asmd = nullptr, *asm_own = nullptr;
   double *work = nullptr;                        // factor slab for large blocks
   unsigned long long *progress = nullptr;        // one counter per CTA of a sweep
   int *abort = nullptr;
@@ -168,8 +171,9 @@ struct Ctx {
   double *sf = nullptr;    // n*4q lift scalars B
   double *contrib = nullptr;  // n*4t per-cell face contributions
   // Schur panels C_s X_o of every cell, column-major t x t: the 4 diagonal
-  // ones (s = o, the Jacobi blocks) or, where schur_panels_full(q), all 16
-  // ([cell][s][o]), which the Schur action then streams instead of X
+  // ones (s = o, the Jacobi blocks) or, where geo.npan == 16
+  // (schur_panels_full(q), or element/full assembly), all 16 ([cell][s][o]),
+  // which the Schur action then streams instead of X
   double *panels = nullptr;
   double *rhs = nullptr, *lam = nullptr, *tmp_trace = nullptr;  // nl
   double *work_cell = nullptr;  // global LU workspace for large cells
@@ -206,7 +210,7 @@ struct Ctx {
   // mixed precision: FP32 copies of X, of the Schur block-Jacobi inverses and
   // of D, and the FP32 Krylov workspace of the inner Schur solve
   // mixed precision: Xf is the FP32 copy of X, or of the 16 Schur panels per
-  // cell where schur_panels_full(q)
+  // cell where geo.npan == 16
   float *Xf = nullptr, *pcf = nullptr, *Df = nullptr, *contribf = nullptr;
   float *kfV = nullptr, *kfw = nullptr, *kfz = nullptr, *kfres = nullptr, *kfcomb = nullptr,
         *kfcorr = nullptr, *kfx = nullptr, *kfrhs = nullptr;
@@ -256,6 +260,11 @@ void upload_desc(Ctx &c, const eg_desc &d);
 // condensation; x = ILU^{-1} b.
 void ilu_refresh(Ctx &c, int form, bool factor);
 void launch_ilu_apply(Ctx &c, int form, const double *b, double *x);
+// ---- element/full assembly (eg_ilu.cu) ----
+// Fill the assembled block-sparse operator of `form` (the ILU(0) block
+// structure, unfactored) at the current state / condensation; y = A x.
+void assemble_blocks(Ctx &c, int form);
+void launch_assembled_apply(Ctx &c, int form, const double *x, double *y);
 // ---- mixed precision (eg_mixed.cu) ----
 // FP32 copies of the condensed responses and of the factored Schur
 // block-Jacobi inverses (after eg_condense and the FP64 factor).

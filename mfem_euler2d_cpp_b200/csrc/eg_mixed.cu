@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(128)
 }
 
 // FP32 Schur action from FP32 copies of the 16 panels C_s X_o of a cell
-// (degrees with schur_panels_full; the FP64 panel form is panel_gemv_kernel).
+// (wherever all 16 panels are kept; the FP64 panel form is panel_gemv_kernel).
 template <int Q>
 __global__ void __launch_bounds__(((16 * Q + 31) / 32) * 32)
     panel_gemv_f32_kernel(Geo g, const float *__restrict__ panels, const float *__restrict__ v,
@@ -182,14 +182,14 @@ struct MixedHdgOps : LinearOpsT<float> {
   void apply(Ctx &c, const float *x, float *y) override {
     ProfScope ps(c, EG_K_SCHUR_APPLY, 2);
     const int grid = std::min(c.n, sm_count_mixed() * 16);
-    if (schur_panels_full(c.q)) {  // Xf holds the FP32 panels
+    if (c.geo.npan == 16) {  // Xf holds the FP32 panels
       switch (c.q) {
 #define EG_PGF(QQ)                                                                                    \
   case QQ:                                                                                            \
     panel_gemv_f32_kernel<QQ><<<grid, ((16 * QQ + 31) / 32) * 32, 0, c.stream>>>(c.geo, c.Xf, x, c.contribf, \
                                                                                 c.skip);              \
     break;
-        EG_PGF(5) EG_PGF(6) EG_PGF(7) EG_PGF(8) EG_PGF(9)
+        EG_PGF(1) EG_PGF(2) EG_PGF(3) EG_PGF(4) EG_PGF(5) EG_PGF(6) EG_PGF(7) EG_PGF(8) EG_PGF(9)
 #undef EG_PGF
         default:
           fail(EG_ERR_INVALID, "unsupported degree");
@@ -225,8 +225,8 @@ void ensure_mixed(Ctx &c) {
   if (c.Xf) return;
   c.ensure_krylov();  // fixes the restart length both solvers use
   // FP32 copy of X, or of the 16 Schur panels per cell where the FP64 Schur
-  // action streams those (schur_panels_full)
-  c.Xf = c.alloc_n<float>((size_t)c.n * (schur_panels_full(c.q) ? 16 * c.t * c.t : c.m * 4 * c.t));
+  // action streams those (all 16 panels kept per cell)
+  c.Xf = c.alloc_n<float>((size_t)c.n * (c.geo.npan == 16 ? 16 * c.t * c.t : c.m * 4 * c.t));
   c.pcf = c.alloc_n<float>((size_t)c.nf * c.t * c.t);
   c.Df = c.alloc_n<float>(c.nl);
   c.contribf = c.alloc_n<float>((size_t)c.n * 4 * c.t);
@@ -246,7 +246,7 @@ void ensure_mixed(Ctx &c) {
 void mixed_prepare(Ctx &c) {
   ensure_mixed(c);
   ProfScope ps(c, EG_K_VECTOR, 3);
-  if (schur_panels_full(c.q)) {
+  if (c.geo.npan == 16) {
     const long long npan = (long long)c.n * 16 * c.t * c.t;
     to_f32_kernel<<<vgrid(npan), 256, 0, c.stream>>>(npan, c.panels, c.Xf);
   } else {

@@ -121,7 +121,7 @@ Options parse(int argc, char **argv) {
                    "--form dg|hdg|both --integrator ssp-dirk3|be\n"
                    "--solver gmres\n"
                    "--precond block-jacobi|block-ilu0 --ilu-ordering none\n"
-                   "--assembly partial --matrix-free --safety 1.1\n"
+                   "--assembly full|element|partial --matrix-free --safety 1.1\n"
                    "--linear-tol E --restart N --max-krylov N --output PREFIX\n"
                    "--check-update --timing-only --no-save-solution --hdg-first\n"
                    "--device cuda --precision fp64|mixed\n";
@@ -172,7 +172,7 @@ Options parse(int argc, char **argv) {
   require(o.device == "cuda", "This executable is the --device cuda path; use the reference euler2d for CPU runs");
   require(o.precision == "fp64" || o.precision == "mixed", "Invalid precision");
   require(o.solver == "gmres", "--solver direct/dense is not available with --device cuda");
-  require(o.assembly == "partial", "--assembly full/element is not available with --device cuda");
+  require(o.precision == "fp64" || o.assembly != "full", "--precision mixed requires --assembly partial or element");
   require(o.ilu_ordering == "none", "--ilu-ordering mdf is not available with --device cuda");
   require(!o.verify, "--verify is a CPU diagnostic of the reference build");
   return o;
@@ -196,7 +196,8 @@ FormResult run_form(const Options &o, const eg_desc &desc, const std::string &fo
   eg_opts_default(&eo);
   eo.form = form == "dg" ? EG_FORM_DG : EG_FORM_HDG;
   eo.precond = o.precond == "block-ilu0" ? EG_PC_BLOCK_ILU0 : EG_PC_BLOCK_JACOBI;
-  eo.assembly = EG_ASSEMBLY_PARTIAL;
+  eo.assembly = o.assembly == "full" ? EG_ASSEMBLY_FULL
+                : o.assembly == "element" ? EG_ASSEMBLY_ELEMENT : EG_ASSEMBLY_PARTIAL;
   eo.precision = o.precision == "mixed" ? EG_PRECISION_MIXED : EG_PRECISION_FP64;
   eo.restart = o.restart;
   eo.max_krylov = o.max_krylov;

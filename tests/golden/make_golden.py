@@ -10,10 +10,11 @@ compiled against the MFEM-subset shim. Two kinds of fixture are written:
   condensation (X, y, rhs, D), Schur action and blocks, recovery and one
   weighted GMRES solve per form, all on a seeded perturbed simple-wave state;
 * cli_*.npz    -- the reference euler2d command line on the configurations
-  its own tests and the headline 16x16 Q3 workload use: final coefficients
-  per form and the per-update _iterations.csv columns.
+  its own tests and the headline 16x16 Q3 workload use, plus element and
+  full assembly: final coefficients per form and the per-update
+  _iterations.csv columns.
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [--only CLI_CASE ...]
 """
 from __future__ import annotations
 
@@ -222,6 +223,15 @@ CLI_CASES = {
     "be_converged_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--cfl", ".1", "--steps", "1",
                             "--integrator", "be", "--form", "both", "--check-update",
                             "--newton-tol", "1e-12", "--linear-tol", "1e-12"],
+    # element and full assembly (src/options.cpp:130-146): element-assembled
+    # operators applied matrix-free, and GMRES on the assembled CSR matrix
+    "element_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "30", "--cfl", "1",
+                       "--steps", "1", "--newton-steps", "2", "--form", "both", "--assembly", "element"],
+    "full_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "30", "--cfl", "1",
+                    "--steps", "1", "--newton-steps", "2", "--form", "both", "--assembly", "full"],
+    "full_ilu_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "30", "--cfl", "1",
+                        "--steps", "1", "--newton-steps", "2", "--form", "both", "--assembly", "full",
+                        "--precond", "block-ilu0"],
 }
 ITER_COLS = ["step", "stage", "newton", "time", "dt", "cfl", "residual_physical_rms", "damping",
              "krylov_iterations", "linear_relative_residual", "dg_linear_relative_residual",
@@ -271,6 +281,18 @@ def main():
     if not (REF / "libeuler_ref.so").exists():
         sys.exit("oracle/_ref is not built: run `make -C oracle` where the reference is available")
     lib = load_ref()
+    only = sys.argv[sys.argv.index("--only") + 1:] if "--only" in sys.argv else None
+    if only:  # regenerate just the named command-line cases (and the manifest)
+        exe = ref_cli()
+        for name in only:
+            data = make_cli(exe, name, CLI_CASES[name])
+            data["u0"] = ref_initial_state(lib, CLI_CASES[name])
+            np.savez_compressed(HERE / f"cli_{name}.npz", **data)
+            print("cli", name)
+        meta = json.loads((HERE / "manifest.json").read_text())
+        meta["cli_cases"] = CLI_CASES
+        (HERE / "manifest.json").write_text(json.dumps(meta, indent=1))
+        return
     rng = np.random.default_rng(20261203)
     for nx, ny, k, alpha, dense in UNIT_CASES:
         data = make_unit(lib, nx, ny, k, alpha, dense, rng)

@@ -72,6 +72,9 @@ def _cli(*args):
     (["--nx"], "Missing option value"),
     (["--volume-order", "5"], "Volume rule must be (k+1)^2 GL points (order 2k+1)"),
     (["--device", "cpu"], "This executable is the --device cuda path"),
+    (["--assembly", "csr"], "Invalid assembly"),
+    (["--solver", "direct", "--assembly", "element"], "Direct LU requires --assembly full"),
+    (["--assembly", "full", "--precision", "mixed"], "--precision mixed requires --assembly partial or element"),
 ])
 def test_cli_rejects_invalid_options(args, message):
     proc = _cli(*args)
@@ -84,3 +87,4 @@ def test_cli_help():
     proc = _cli("--help")
     assert proc.returncode == 0
     assert "--form dg|hdg|both" in proc.stdout
+    assert "--assembly full|element|partial" in proc.stdout

@@ -67,6 +67,9 @@ def test_cli_matches_reference(path, tmp_path):
             assert abs(s[name] - rs[name]) <= 1e-9 * rs[name] + 1e-15
         assert s["max_conservation_drift"] < 1e-12
         assert summary["device"] == "cuda"
+        assembly = args[args.index("--assembly") + 1] if "--assembly" in args else "partial"
+        assert summary["assembly"] == assembly
+        assert int(summary["matrix_free"]) == (assembly != "full")  # src/options.cpp:135
     with open(f"{prefix}_comparison.csv", newline="") as fh:
         comp = next(csv.DictReader(fh))
     assert float(comp["max_nodal_difference"]) < 1e-8

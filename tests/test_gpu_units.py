@@ -17,9 +17,9 @@ OP_TOL = 1e-12
 SOLVE_TOL = 1e-10
 
 
-def _ctx(f, form):
+def _ctx(f, form, **opts):
     d = capi.simple_wave_desc(int(f["nx"]), int(f["ny"]), int(f["k"]), float(f["alpha"]))
-    ctx = capi.Context(d, capi.default_opts(form=form))
+    ctx = capi.Context(d, capi.default_opts(form=form, **opts))
     ctx.upload("U", f["u"])
     rate = ctx.freeze(float(f["dt"]), check_admissible=True)
     ctx.upload("OLD", f["old"])
@@ -93,6 +93,53 @@ def test_hdg_linear_solve(unit):
         assert rel_err(x, f["solve_hdg_x"]) < SOLVE_TOL
         assert abs(st.count - int(f["solve_hdg_count"][0])) <= 1
         assert st.residual <= 1e-11
+
+
+@pytest.mark.parametrize("assembly", [capi.ASSEMBLY_ELEMENT, capi.ASSEMBLY_FULL], ids=["element", "full"])
+def test_assembled_operators_and_solves(unit, assembly):
+    """--assembly element|full: the Schur action from the per-cell entries C X
+    (all 16 panels kept at every degree), the Schur blocks read from that
+    layout, and the DG and HDG solves (GMRES on the assembled block-sparse
+    matrix for full assembly, on the element operators for element
+    assembly) against the reference's matrix-free solves."""
+    f = unit
+    ctx, _ = _ctx(f, capi.FORM_HDG, assembly=assembly)
+    with ctx:
+        ctx.upload("R", f["r"])
+        ctx.condense()
+        assert rel_err(ctx.schur_apply(f["v"]), f["sv"]) < OP_TOL
+        if "schur_blocks" in f:
+            ctx.pc_factor(False)
+            assert rel_err(ctx.download("PC_BLOCKS"), f["schur_blocks"]) < OP_TOL
+        x, _, st = ctx.linear_solve(f["rhs"])
+        assert rel_err(x, f["solve_hdg_x"]) < SOLVE_TOL
+        assert abs(st.count - int(f["solve_hdg_count"][0])) <= 1
+        assert st.residual <= 1e-11
+    ctx, _ = _ctx(f, capi.FORM_DG, assembly=assembly)
+    with ctx:
+        x, _, st = ctx.linear_solve(-f["r"])
+        assert rel_err(x, f["solve_dg_x"]) < SOLVE_TOL
+        assert abs(st.count - int(f["solve_dg_count"][0])) <= 1
+        assert st.residual <= 1e-11
+
+
+def test_full_assembly_with_block_ilu(unit):
+    """Full assembly keeps the assembled matrix apart from the ILU(0) factors."""
+    f = unit
+    for form in (capi.FORM_DG, capi.FORM_HDG):
+        ctx, _ = _ctx(f, form, assembly=capi.ASSEMBLY_FULL, precond=capi.PC_ILU0)
+        with ctx:
+            if form == capi.FORM_HDG:
+                ctx.upload("R", f["r"])
+                ctx.condense()
+                x, _, st = ctx.linear_solve(f["rhs"])
+                want, count = f["solve_hdg_ilu_x"], int(f["solve_hdg_ilu_count"][0])
+            else:
+                x, _, st = ctx.linear_solve(-f["r"])
+                want, count = f["solve_dg_ilu_x"], int(f["solve_dg_ilu_count"][0])
+            assert rel_err(x, want) < SOLVE_TOL
+            assert abs(st.count - count) <= 1
+            assert st.residual <= 1e-11
 
 
 def test_pc_apply_inverts_blocks(unit):
