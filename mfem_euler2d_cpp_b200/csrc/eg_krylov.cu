@@ -590,7 +590,8 @@ double gmres_t(Ctx &c, LinearOpsT<T> &ops, const KrylovBufs<T> &kb, const T *rhs
 double gmres(Ctx &c, LinearOps &ops, const double *rhs, double *x, double tol, int limit,
              bool zero_guess, int *count, double *rhs_norm_out, double known_rhs_norm) {
   c.ensure_krylov();
-  const KrylovBufs<double> kb{c.V, c.kw, c.kz, c.kres, c.kcomb, c.kcorr, (size_t)c.kN, c.kR};
+  // columns of the operator's own length, contiguous
+  const KrylovBufs<double> kb{c.V, c.kw, c.kz, c.kres, c.kcomb, c.kcorr, (size_t)ops.N, c.kR};
   return gmres_t<double>(c, ops, kb, rhs, x, tol, limit, zero_guess, true, count, rhs_norm_out, known_rhs_norm);
 }
 
