@@ -183,7 +183,9 @@ void *eg_stream(eg_ctx *ctx);
  * box, gas, tables): the device buffers are kept, the state must be set anew.
  * No counterpart in the reference (one Problem per run). */
 int eg_set_desc(eg_ctx *ctx, const eg_desc *d);
-/* Change solver options between updates (form, preconditioner, tolerance). */
+/* Change solver options between updates (form, preconditioner, tolerance).
+ * The assembly mode is fixed when the context is created (it decides how many
+ * Schur panels the condensation keeps); a different one is EG_ERR_INVALID. */
 int eg_set_opts(eg_ctx *ctx, const eg_opts *o);
 /* Sizes: n, p, m, t, nf, nu, nl. */
 int eg_sizes(const eg_ctx *ctx, int out[7]);
