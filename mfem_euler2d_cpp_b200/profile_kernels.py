@@ -20,6 +20,7 @@ from . import capi
 OPS = ("condense", "schur_apply", "recover", "pc_factor", "pc_apply", "dg_apply", "residual",
        "linear_solve", "dg_jacobi")
 PRECONDS = {"block-jacobi": capi.PC_JACOBI, "block-ilu0": capi.PC_ILU0}
+ASSEMBLY = {"partial": capi.ASSEMBLY_PARTIAL, "element": capi.ASSEMBLY_ELEMENT, "full": capi.ASSEMBLY_FULL}
 
 
 def main(argv=None):
@@ -32,6 +33,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--precond", choices=sorted(PRECONDS), default="block-jacobi")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--assembly", choices=sorted(ASSEMBLY), default="partial")
     ap.add_argument("--form", choices=("dg", "hdg"), default=None,
                     help="form of the context (default: dg for dg_apply/dg_jacobi, hdg otherwise)")
     args = ap.parse_args(argv)
@@ -42,7 +44,9 @@ def main(argv=None):
         form = capi.FORM_DG if args.form == "dg" else capi.FORM_HDG
     d = capi.simple_wave_desc(args.nx, args.ny, args.k, args.alpha)
     prec = capi.PRECISION_MIXED if args.precision == "mixed" else capi.PRECISION_FP64
-    with capi.Context(d, capi.default_opts(form=form, precond=PRECONDS[args.precond], precision=prec)) as ctx:
+    opts = capi.default_opts(form=form, precond=PRECONDS[args.precond], precision=prec,
+                             assembly=ASSEMBLY[args.assembly])
+    with capi.Context(d, opts) as ctx:
         ctx.initial()
         rate = ctx.freeze(1e-3)
         dt = 0.24169426078821 / rate  # first SSP-DIRK3 stage at CFL 1
@@ -78,13 +82,14 @@ def main(argv=None):
             elif args.op == "residual":
                 ctx.residual()
             elif args.op == "linear_solve":
-                _, _, st = ctx.linear_solve(ctx.download("RHS"))
+                rhs = ctx.download("RHS") if form == capi.FORM_HDG else -ctx.download("R")
+                _, _, st = ctx.linear_solve(rhs)
                 out_counts.append(st.count)
         names = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "recover",
                  "recovered_residual", "schur_jacobi", "pc_apply", "krylov", "freeze", "admissible",
                  "vector"]
         out = {"op": args.op, "nx": args.nx, "ny": args.ny, "k": args.k, "reps": args.reps,
-               "precond": args.precond, "precision": args.precision}
+               "precond": args.precond, "precision": args.precision, "assembly": args.assembly}
         if out_counts:
             out["krylov_counts"] = out_counts
         for i, name in enumerate(names):
