@@ -59,8 +59,13 @@ enum eg_status {
   EG_ERR_UPDATE_EQUATION = 22,  /* "Independent recovered DG equation check failed" stepper.cpp:190 */
   EG_ERR_UPDATE_EQUIVALENCE = 23, /* "DG/HDG one-update equivalence failed" stepper.cpp:197 */
   EG_ERR_WAIT_LIMIT = 24,       /* a bounded device-side wait of a dependency-driven sweep gave up
-                                   (no counterpart in the reference, which runs the sweep serially) */
-  EG_ERR_COUNT = 25
+                                   (no counterpart in the reference, which runs the sweep serially);
+                                   the context stays usable */
+  EG_ERR_CONTEXT_LOST = 25,     /* after a wait gave up, a bulk copy of the aborted sweep did not
+                                   land within its own bound either: the context's device memory
+                                   can no longer be trusted, every later call on it returns this
+                                   status, and only eg_destroy is valid (no reference counterpart) */
+  EG_ERR_COUNT = 26
 };
 
 enum eg_form { EG_FORM_DG = 0, EG_FORM_HDG = 1 };
@@ -381,18 +386,23 @@ void eg_server_destroy(eg_server *s);
  * cannot create an eg_ctx, because a context allocates its buffers.
  *
  * r must point to n*m doubles of device-accessible memory laid out as the
- * reference's body vectors (host pointers are rejected with EG_ERR_INVALID);
+ * reference's body vectors, on the current device (host pointers and memory
+ * of another device are rejected with EG_ERR_INVALID, as is a descriptor that
+ * eg_create would refuse: non-lexicographic nodes or a non-positive area);
  * *out receives sqrt(sum_i area * mass_i * r_i^2), the same value eg_cell_norm
- * returns for the same vector. stream may be NULL (the default stream); the
- * call returns after the result is on the host.
+ * returns for the same vector. stream may be NULL (the default stream).
+ *
+ * The call is synchronous: it copies the metric table from the host, runs the
+ * reduction and waits on the stream for the result, so it must not be called
+ * while its stream is being captured into a CUDA graph.
  *
  * Scratch: a fixed 4 KB static device array inside the library (partial sums,
  * completion counter, metric table), held by every GPU that loads the library
  * until the process exits. Degrees k > 8 exceed its metric table and are
  * rejected with EG_ERR_INVALID. The first call on each device looks up the
- * array's device address; make that first call before any stream capture.
- * All calls on a device share the array, so calls that overlap on the GPU
- * (concurrent streams or threads) race and must be serialised by the caller. */
+ * array's device address with that device current. All calls on a device
+ * share the array, so calls that overlap on the GPU (concurrent streams or
+ * threads) race and must be serialised by the caller. */
 int eg_cell_norm_noalloc(const eg_desc *d, const double *r, void *stream, double *out);
 
 /* ------------------------------------------------------------ profiling */
@@ -411,6 +421,19 @@ int eg_profile_reset(eg_ctx *ctx);
 int eg_profile_query(eg_ctx *ctx, int kernel_class, double *ms, long long *launches);
 /* Total kernels launched on the context since creation. */
 long long eg_launch_count(const eg_ctx *ctx);
+
+/* y[i] = the condensation's pivot reciprocal of x[i] (host arrays of n
+ * values), for tests that bound it against IEEE division (no reference
+ * counterpart: the reference divides by each pivot). */
+int eg_check_pivot_reciprocal(const double *x, double *y, long long n);
+
+/* Test setting of the block ILU(0) device waits (no reference counterpart:
+ * the reference's factor and sweeps are serial). limit_ns bounds every wait
+ * of the factor and the sweeps (0 restores the default, 250 ms); starve != 0
+ * makes every wait on another CTA unreachable, so that the next factor or
+ * apply runs out its bound, returns EG_ERR_WAIT_LIMIT and leaves the context
+ * usable. Applies to both forms' plans, including ones built later. */
+int eg_set_ilu_wait(eg_ctx *ctx, unsigned long long limit_ns, int starve);
 
 #ifdef __cplusplus
 }

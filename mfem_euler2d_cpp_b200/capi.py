@@ -31,6 +31,7 @@ STATUS_NAMES = {
     16: "EG_ERR_LINE_SEARCH", 17: "EG_ERR_OUT_OF_MEMORY", 18: "EG_ERR_STEP_INTERVAL",
     19: "EG_ERR_NEWTON_CONVERGE", 20: "EG_ERR_DIRK_INADMISSIBLE", 21: "EG_ERR_INITIAL",
     22: "EG_ERR_UPDATE_EQUATION", 23: "EG_ERR_UPDATE_EQUIVALENCE", 24: "EG_ERR_WAIT_LIMIT",
+    25: "EG_ERR_CONTEXT_LOST",
 }
 FORM_DG, FORM_HDG = 0, 1
 PC_JACOBI, PC_ILU0 = 0, 1
@@ -151,6 +152,8 @@ def load() -> C.CDLL:
         "eg_profile_reset": (C.c_int, [vp]),
         "eg_profile_query": (C.c_int, [vp, C.c_int, _DP, C.POINTER(C.c_longlong)]),
         "eg_launch_count": (C.c_longlong, [vp]),
+        "eg_set_ilu_wait": (C.c_int, [vp, C.c_ulonglong, C.c_int]),
+        "eg_check_pivot_reciprocal": (C.c_int, [_DP, _DP, C.c_longlong]),
         "eg_cell_norm_noalloc": (C.c_int, [C.POINTER(Desc), C.c_void_p, C.c_void_p, _DP]),
         "eg_create": (C.c_int, [C.POINTER(Desc), C.POINTER(Opts), C.POINTER(vp)]),
         "eg_destroy": (None, [vp]),
@@ -334,6 +337,10 @@ class Context:
         count = C.c_longlong()
         self._check(self.lib.eg_pc_size(self.h, C.byref(count)))
         return count.value
+
+    def set_ilu_wait(self, limit_ns: int = 0, starve: bool = False):
+        """Test setting of the block ILU(0) device waits (eg_set_ilu_wait)."""
+        self._check(self.lib.eg_set_ilu_wait(self.h, int(limit_ns), int(starve)))
 
     def pc_factor(self, factor: bool = True):
         self._check(self.lib.eg_pc_factor(self.h, int(factor)))

@@ -50,6 +50,7 @@ static const char *kMessages[EG_ERR_COUNT] = {
     "Independent recovered DG equation check failed",
     "DG/HDG one-update equivalence failed",
     "device wait limit reached",
+    "context lost: a bulk copy of an aborted sweep did not finish; destroy the context",
 };
 
 void *Ctx::alloc(size_t nbytes) {
@@ -112,7 +113,12 @@ void Ctx::prof_resolve() {
 
 void Ctx::check_device_error() {
   EG_CUDA(cudaMemcpyAsync(herr, derr, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  EG_CUDA(cudaMemcpyAsync(herr + 2, derr + 2, sizeof(int), cudaMemcpyDeviceToHost, stream));
   sync();
+  if (herr[2]) {
+    broken = true;
+    fail(EG_ERR_CONTEXT_LOST, kMessages[EG_ERR_CONTEXT_LOST]);
+  }
   const int code = *herr;
   if (code != 0) {
     EG_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), stream));
@@ -473,6 +479,10 @@ static thread_local std::string g_create_error;
 
 template <class F>
 static int guard(eg_ctx *ctx, F &&f) {
+  if (ctx && ctx->c.broken) {
+    ctx->c.err = eg::kMessages[EG_ERR_CONTEXT_LOST];
+    return EG_ERR_CONTEXT_LOST;
+  }
   try {
     f();
     return EG_OK;
@@ -942,6 +952,18 @@ int eg_errors(eg_ctx *ctx, double time, double out[4]) {
     std::vector<double> u(c.nu);
     eg::download_vec(c, u.data(), c.u, c.nu);
     eg::host::errors(c.desc, u.data(), time, out);
+  });
+}
+
+int eg_set_ilu_wait(eg_ctx *ctx, unsigned long long limit_ns, int starve) {
+  if (!ctx) return EG_ERR_INVALID;
+  return guard(ctx, [&] {
+    ctx->c.ilu_wait_limit_ns = limit_ns ? limit_ns : eg::kIluWaitLimitNs;
+    ctx->c.ilu_starve = starve != 0;
+    for (auto &P : ctx->c.ilu) {
+      P.wait_limit_ns = ctx->c.ilu_wait_limit_ns;
+      P.starve = ctx->c.ilu_starve;
+    }
   });
 }
 

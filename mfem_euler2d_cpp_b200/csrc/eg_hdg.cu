@@ -206,8 +206,12 @@ __device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, do
 
 // Reciprocal of a pivot: hardware estimate refined by two Newton-Raphson
 // steps r <- r + r (1 - x r) (quadratic convergence from the ~2^-20 estimate;
-// result within one unit in the last place of 1/x).
+// result within one unit in the last place of 1/x). The estimate flushes
+// subnormal inputs and results to zero, so magnitudes outside
+// [2^-1020, 2^1020] (and zero, infinities, NaN) take IEEE division instead.
 __device__ __forceinline__ double pivot_reciprocal(double x) {
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-1020 && ax <= 0x1p+1020)) return 1.0 / x;
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
   double e = fma(-x, r, 1.0);
@@ -1237,3 +1241,35 @@ void launch_schur_jacobi(Ctx &c, bool factor) {
 }
 
 }  // namespace eg
+
+// Element-wise pivot_reciprocal of n values (host arrays), for the test that
+// bounds it against IEEE division.
+namespace eg {
+namespace {
+__global__ void pivot_reciprocal_kernel(long long n, const double *__restrict__ x, double *__restrict__ y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = pivot_reciprocal(x[i]);
+}
+}  // namespace
+}  // namespace eg
+
+extern "C" int eg_check_pivot_reciprocal(const double *x, double *y, long long n) {
+  if (!x || !y || n <= 0) return EG_ERR_INVALID;
+  double *d = nullptr;
+  if (cudaMalloc(&d, sizeof(double) * 2 * (size_t)n) != cudaSuccess) {
+    cudaGetLastError();
+    return EG_ERR_OUT_OF_MEMORY;
+  }
+  cudaError_t e = cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    eg::pivot_reciprocal_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 1024), 256>>>(n, d, d + n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(y, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return EG_ERR_CUDA;
+  }
+  return EG_OK;
+}

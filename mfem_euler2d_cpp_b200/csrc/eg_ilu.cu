@@ -18,9 +18,11 @@
 // (forward, factor) or decreasing (backward) order. A CTA publishes how many
 // of its rows are final in one 64-bit counter tagged with the launch's epoch;
 // a row waits only for rows earlier in the sweep order, which co-resident
-// CTAs own, so no wait can depend on itself. Every wait is bounded: on
-// timeout the kernel records DERR_WAIT_LIMIT, sets the abort word, and all
-// CTAs leave at their next wait (after their own bulk copies have landed).
+// CTAs own, so no wait can depend on itself. Every wait is bounded in time
+// (IluPlan::wait_limit_ns, far above the longest legitimate wait, which a
+// whole factor or sweep bounds): on timeout the kernel records
+// DERR_WAIT_LIMIT, sets the abort word, and all CTAs leave at their next wait
+// (after their own bulk copies have landed).
 //
 // The factor stores the explicit inverse of each factored diagonal block
 // (pivoted LU applied to the identity), so RightSolve becomes a product with
@@ -35,8 +37,8 @@
 namespace eg {
 namespace {
 
-constexpr unsigned kSpinLimit = 1u << 24;  // polls per wait, each with a short sleep
-constexpr unsigned kCopySpinLimit = 1u << 16;  // try_wait itself suspends between polls
+constexpr unsigned kCopySpinLimit = 1u << 16;   // try_wait itself suspends between polls
+constexpr unsigned kDrainSpinLimit = 1u << 24;  // abort path: let an issued copy land
 constexpr int kStageBlocks = 4;             // blocks staged per warp and row
 constexpr int kStageMaxB = 36;              // larger blocks are read from global memory
 constexpr size_t kSweepSmemBudget = 210 * 1024;
@@ -54,28 +56,54 @@ __device__ __forceinline__ void give_up(int *abort, int *err) {
   atomicExch(abort, 1);
   raise_err(err, DERR_WAIT_LIMIT);
 }
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits are bounded in time: a wait that has polled for more than limit_ns
+// nanoseconds (read every 64 polls from the global timer) gives up.
 // Bounded wait until *p >= target (another CTA's progress).
-__device__ bool wait_progress(const unsigned long long *p, unsigned long long target, int *abort, int *err) {
-  for (unsigned it = 0; it < kSpinLimit; ++it) {
+__device__ bool wait_progress(const unsigned long long *p, unsigned long long target, int *abort, int *err,
+                              unsigned long long limit_ns) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
     if (ld_acquire(p) >= target) return true;
     if (ld_volatile(abort)) return false;
     if (it >= 16) __nanosleep(64);
+    if ((it & 63u) == 0) {
+      const unsigned long long now = global_ns();
+      if (it == 0) t0 = now;
+      else if (now - t0 > limit_ns) break;
+    }
   }
   give_up(abort, err);
   return false;
 }
 // Bounded wait until the CTA's own published row count reaches target.
-__device__ bool wait_local(const volatile unsigned *count, unsigned target, int *abort, int *err) {
-  for (unsigned it = 0; it < kSpinLimit; ++it) {
+__device__ bool wait_local(const volatile unsigned *count, unsigned target, int *abort, int *err,
+                           unsigned long long limit_ns) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
     if (*count >= target) return true;
     if (ld_volatile(abort)) return false;
     if (it >= 16) __nanosleep(32);
+    if ((it & 63u) == 0) {
+      const unsigned long long now = global_ns();
+      if (it == 0) t0 = now;
+      else if (now - t0 > limit_ns) break;
+    }
   }
   give_up(abort, err);
   return false;
 }
+// The progress value a wait needs: `starve` (a test setting) asks for one no
+// CTA ever publishes, so every wait on another CTA runs out.
+__device__ __forceinline__ unsigned long long need(unsigned long long tag, int slot, int starve) {
+  return starve ? ~0ull : (tag | (unsigned long long)(slot + 1));
+}
 
-// mbarrier + bulk copy (TMA, no multicast) into this CTA's shared memory.
+// mbarrier + bulk copy (cp.async.bulk, this CTA only) into its shared memory.
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
@@ -103,8 +131,8 @@ __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parit
       : "memory");
   return ok != 0;
 }
-__device__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-  for (unsigned it = 0; it < kCopySpinLimit; ++it)
+__device__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit) {
+  for (unsigned it = 0; it < limit; ++it)
     if (mbar_try(bar, parity)) return true;
   return false;
 }
@@ -136,6 +164,8 @@ struct SweepArgs {
   int *abort, *err;
   unsigned long long tag;
   int staged;        // stage up to kStageBlocks blocks per row in shared memory
+  unsigned long long limit_ns;  // bound of every wait
+  int starve;        // test setting: waits on other CTAs can never be met
 };
 
 // FixedBlockILU::Mult (src/block_ilu.cpp:88-109). Forward: w_i = b_i -
@@ -197,9 +227,12 @@ __global__ void __launch_bounds__(256, 1) ilu_sweep_kernel(SweepArgs a) {
       acc[s] = r < B ? __ldcg(a.in + (size_t)i * B + r) : 0.;
     }
     if (copy) {
-      if (!mbar_wait(&bars[warp], phase)) {
+      if (!mbar_wait(&bars[warp], phase, kCopySpinLimit)) {
         give_up(a.abort, a.err);
-        mbar_wait(&bars[warp], phase);  // let the copy land before the CTA can exit
+        // let the copy land before the CTA can exit; if even the longer drain
+        // bound runs out, the copy may still write this CTA's shared memory:
+        // err[2] tells the host that the context can no longer be trusted
+        if (!mbar_wait(&bars[warp], phase, kDrainSpinLimit) && lane == 0) atomicExch(a.err + 2, 1);
         return;
       }
       phase ^= 1u;
@@ -210,8 +243,8 @@ __global__ void __launch_bounds__(256, 1) ilu_sweep_kernel(SweepArgs a) {
       if (k < ne && ok) {
         const int owner = dep[k].x >> kOwnerShift, js = dep[k].x & kSlotMask, j = dep[k].y;
         const bool local = owner == g;
-        ok = local ? wait_local(dl, (unsigned)js + 1, a.abort, a.err)
-                   : wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
+        ok = local ? wait_local(dl, (unsigned)js + 1, a.abort, a.err, a.limit_ns)
+                   : wait_progress(a.progress + owner, need(a.tag, js, a.starve), a.abort, a.err, a.limit_ns);
         if (ok) {
           __threadfence_block();
           const bool in_ring = local && slot - js <= a.ring - W;
@@ -265,7 +298,7 @@ __global__ void __launch_bounds__(256, 1) ilu_sweep_kernel(SweepArgs a) {
     __syncwarp();
     int pub = 1;
     if (lane == 0) {
-      pub = wait_local(dl, (unsigned)slot, a.abort, a.err);  // rows are published in order
+      pub = wait_local(dl, (unsigned)slot, a.abort, a.err, a.limit_ns);  // rows are published in order
       if (pub) {
         *dl = (unsigned)slot + 1;
         publish_max(a.progress + g, a.tag | (unsigned long long)(slot + 1));
@@ -286,6 +319,8 @@ struct FactorArgs {
   unsigned long long *progress;
   int *abort, *err;
   unsigned long long tag;
+  unsigned long long limit_ns;  // bound of every wait
+  int starve;                   // test setting: waits on other CTAs can never be met
 };
 
 // FixedBlockILU::Factor (src/block_ilu.cpp:74-87), one CTA per row: for each
@@ -322,7 +357,8 @@ __global__ void __launch_bounds__(256, 1) ilu_factor_kernel(FactorArgs a) {
       for (int k = 0; k < m.z && ok; ++k) {
         const int2 d = a.deps[(size_t)(p0 + slot) * kMaxDeps + k];
         const int owner = d.x >> kOwnerShift, js = d.x & kSlotMask;
-        if (owner != g) ok = wait_progress(a.progress + owner, a.tag | (unsigned long long)(js + 1), a.abort, a.err);
+        if (owner != g)
+          ok = wait_progress(a.progress + owner, need(a.tag, js, a.starve), a.abort, a.err, a.limit_ns);
       }
       stop = !ok;
     }
@@ -746,6 +782,8 @@ void build_plan(Ctx &c, int form) {
   P.abort = c.alloc_n<int>(1);
   EG_CUDA(cudaMemsetAsync(P.abort, 0, sizeof(int), c.stream));
   P.epoch = 0;
+  P.wait_limit_ns = c.ilu_wait_limit_ns;
+  P.starve = c.ilu_starve;
   P.built = true;
 }
 
@@ -772,6 +810,8 @@ void sweep(Ctx &c, IluPlan &P, const double *in, double *out) {
   a.err = c.derr;
   a.tag = (unsigned long long)(++P.epoch) << 32;
   a.staged = P.staged;
+  a.limit_ns = P.wait_limit_ns;
+  a.starve = P.starve;
   launch_coop(ilu_sweep_kernel<S, BACK>, P.grid_sweep, 32 * P.sweep_warps, P.sweep_smem, c.stream, a);
 }
 
@@ -813,6 +853,8 @@ void factor_launch(Ctx &c, IluPlan &P) {
   a.abort = P.abort;
   a.err = c.derr;
   a.tag = (unsigned long long)(++P.epoch) << 32;
+  a.limit_ns = P.wait_limit_ns;
+  a.starve = P.starve;
   launch_coop(ilu_factor_kernel<RMAX, SMEM>, P.grid_factor, 256, SMEM ? P.factor_smem : 0, c.stream, a);
 }
 
@@ -930,6 +972,8 @@ void launch_ilu_apply(Ctx &c, int form, const double *b, double *x) {
   IluPlan &P = c.ilu[form];
   if (!P.built) fail(EG_ERR_INVALID, "no preconditioner built");
   ProfScope ps(c, EG_K_PC_APPLY, 2);
+  // a sweep that gave up leaves the abort word set; every apply starts clear
+  EG_CUDA(cudaMemsetAsync(P.abort, 0, sizeof(int), c.stream));
   sweep_dispatch<false>(c, P, b, P.w);
   sweep_dispatch<true>(c, P, P.w, x);
 }

@@ -118,6 +118,12 @@ struct KrylovBufs {
   int R;
 };
 
+// Bound of a device-side wait of the block ILU(0) factor and sweeps. The
+// longest legitimate wait is bounded by one whole factor or sweep (45 ms for
+// the factor at 128 x 128 Q4 HDG); 250 ms leaves a wide margin and still ends
+// a wait on a row that never comes within a fraction of a second.
+constexpr unsigned long long kIluWaitLimitNs = 250ull * 1000 * 1000;
+
 // Block ILU(0) of one form (FixedBlockILU, src/block_ilu.cpp:10-109): fixed
 // BSR structure in natural order, numeric blocks and the explicit inverses of
 // the factored diagonal blocks. Built on first use (eg_ilu.cu).
@@ -136,6 +142,10 @@ struct IluPlan {
   unsigned long long *progress = nullptr;        // one counter per CTA of a sweep
   int *abort = nullptr;
   unsigned epoch = 0;
+  // bound of every device-side wait of the factor and the sweeps; starve (a
+  // test setting) makes every wait on another CTA unreachable
+  unsigned long long wait_limit_ns = kIluWaitLimitNs;
+  int starve = 0;
   int grid_factor = 0, grid_sweep = 0, sweep_warps = 0, staged = 0, ring = 0, maxrow = 0, maxupd = 0;
   size_t sweep_smem = 0, factor_smem = 0;
   // sweep schedules (forward, backward): per CTA the first position, per
@@ -206,6 +216,8 @@ struct Ctx {
   bool update_timer_open = false;
 
   IluPlan ilu[2];  // per form (EG_FORM_DG, EG_FORM_HDG)
+  unsigned long long ilu_wait_limit_ns = kIluWaitLimitNs;  // eg_set_ilu_wait
+  int ilu_starve = 0;
   double *step_bufs = nullptr;  // time loop: step state, stage base, 4 slopes (6 nu), reused
   // mixed precision: FP32 copies of X, of the Schur block-Jacobi inverses and
   // of D, and the FP32 Krylov workspace of the inner Schur solve
@@ -217,6 +229,9 @@ struct Ctx {
 
   bool residual_ready = false;
   bool condensed = false;
+  // set when an aborted sweep's bulk copy did not land within its bound: the
+  // context's device memory can no longer be trusted; only eg_destroy works
+  bool broken = false;
   Profiler prof;
   long long launches = 0;
 

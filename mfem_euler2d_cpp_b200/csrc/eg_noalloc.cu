@@ -97,6 +97,10 @@ extern "C" int eg_cell_norm_noalloc(const eg_desc *d, const double *r, void *str
   if (d->k < 0 || d->k > EG_MAX_Q - 1 || d->nx < 2 || d->ny < 2) return EG_ERR_INVALID;
   const int q = d->k + 1, p = q * q, m = 4 * p;
   if (p > EG_MAX_P) return EG_ERR_INVALID;  // metric table capacity of the scratch
+  // the same descriptor checks as eg_create: lexicographic nodes, a positive cell area
+  if (!(d->area > 0.)) return EG_ERR_INVALID;
+  for (int i = 0; i < p; ++i)
+    if (d->tensor_node[i] != i) return EG_ERR_INVALID;
   const long long n = (long long)d->nx * d->ny * m;
   // the vector must be device-accessible memory: a host pointer would fault the kernel
   cudaPointerAttributes attr;
@@ -108,6 +112,13 @@ extern "C" int eg_cell_norm_noalloc(const eg_desc *d, const double *r, void *str
   double *scratch = nullptr;
   const int rc = scratch_address(&scratch);
   if (rc != EG_OK) return rc;
+  // device memory of another GPU is not reachable without peer access: refuse it
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return EG_ERR_CUDA;
+  }
+  if (attr.type == cudaMemoryTypeDevice && attr.device != dev) return EG_ERR_INVALID;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double table[EG_MAX_P];
   for (int i = 0; i < p; ++i) table[i] = d->area * d->mass[i];

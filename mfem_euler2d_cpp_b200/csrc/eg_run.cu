@@ -215,6 +215,10 @@ struct eg_stepper {
 
 template <class F>
 static int guard_run(eg::Ctx &c, F &&f) {
+  if (c.broken) {
+    c.err = eg_status_string(EG_ERR_CONTEXT_LOST);
+    return EG_ERR_CONTEXT_LOST;
+  }
   try {
     f();
     return EG_OK;

@@ -54,3 +54,42 @@ def test_cli_past_shock_time():
                           capture_output=True, text=True, timeout=120)
     assert proc.returncode == 1
     assert "Exact solution requires T < 4/((gamma+1)*pi)" in proc.stderr
+
+
+@pytest.mark.parametrize("form", ["dg", "hdg"])
+def test_ilu_wait_limit_runs_out_and_context_recovers(form):
+    """A block ILU(0) factor and apply whose waits on other CTAs can never be
+    met (a progress value no CTA publishes) run out their 1 ms bound, return
+    EG_ERR_WAIT_LIMIT and leave the context usable: with the default bound
+    restored the same factor and apply give the reference's numbers."""
+    hdg = form == "hdg"
+    nx, ny, k = 12, 10, 2
+    d = capi.simple_wave_desc(nx, ny, k, 35.0)
+    opts = capi.default_opts(form=capi.FORM_HDG if hdg else capi.FORM_DG, precond=capi.PC_ILU0)
+    with capi.Context(d, opts) as ctx:
+        ctx.initial()
+        u = ctx.download("U")
+        dt = 0.02
+        ctx.freeze(dt)
+        ctx.upload("OLD", u * 0.999)
+        ctx.set_dt(dt)
+        ctx.residual()
+        if hdg:
+            ctx.condense()
+        n = ctx.nl if hdg else ctx.nu
+        b = np.cos(0.37 * np.arange(n))
+        ctx.pc_factor(True)
+        good = ctx.pc_apply(b)
+        ctx.set_ilu_wait(limit_ns=1_000_000, starve=True)
+        with pytest.raises(capi.EngineError) as exc:
+            ctx.pc_apply(b)
+        assert exc.value.status == 24
+        with pytest.raises(capi.EngineError) as exc:
+            ctx.pc_factor(True)
+        assert exc.value.status == 24
+        ctx.set_ilu_wait()  # default bound, waits reachable again
+        ctx.pc_factor(True)
+        again = ctx.pc_apply(b)
+        assert np.array_equal(again, good)
+        x, _, st = ctx.linear_solve(-ctx.download("R") if not hdg else ctx.download("RHS"))
+        assert st.residual <= 1e-11 and np.all(np.isfinite(x))

@@ -198,3 +198,30 @@ def test_hdg_jacobi_inverses_download(unit):
         eye = np.broadcast_to(np.eye(t), prod.shape)
         scale = np.abs(s).max(axis=(1, 2)) * np.abs(inv).max(axis=(1, 2))
         assert np.max(np.abs(prod - eye).max(axis=(1, 2)) / scale) < 1e-12
+
+
+def test_pivot_reciprocal_within_one_ulp_of_division():
+    """The condensation's pivot reciprocal (hardware estimate + two
+    Newton-Raphson steps) against IEEE 1/x over every binary exponent of the
+    normal range, both signs, plus the edges the estimate cannot take
+    (subnormal and near-overflow magnitudes, which take IEEE division)."""
+    import ctypes as C
+
+    lib = capi.load()
+    rng = np.random.default_rng(11)
+    exps = np.arange(-1022, 1023)
+    mant = rng.uniform(1.0, 2.0, size=(exps.size, 8))
+    x = np.ldexp(mant, exps[:, None]).ravel()
+    x = np.concatenate([x, -x, [5e-324, -5e-324, 2.2250738585072014e-308 / 3, 1e-310, np.finfo(float).max,
+                                -np.finfo(float).max, 2.0 ** 1021, 2.0 ** -1021, 1.0, -1.0]])
+    y = np.empty_like(x)
+    rc = lib.eg_check_pivot_reciprocal(x.ctypes.data_as(C.POINTER(C.c_double)),
+                                       y.ctypes.data_as(C.POINTER(C.c_double)), x.size)
+    assert rc == capi.OK
+    with np.errstate(over="ignore", divide="ignore"):
+        ref = 1.0 / x
+    finite = np.isfinite(ref) & (ref != 0)
+    ulp = np.spacing(np.abs(ref[finite]))
+    assert np.all(np.abs(y[finite] - ref[finite]) <= ulp)
+    # overflow to infinity and results below the normal range match division exactly
+    assert np.array_equal(y[~finite], ref[~finite])

@@ -46,3 +46,37 @@ def test_noalloc_cell_norm_rejects_host_pointer():
     rc = lib.eg_cell_norm_noalloc(C.byref(desc), C.c_void_p(host.ctypes.data), None, C.byref(out))
     assert rc == 1  # EG_ERR_INVALID
     assert out.value == -1.0
+
+
+def test_noalloc_cell_norm_rejects_descriptors_the_context_refuses():
+    import torch
+
+    lib = capi.load()
+    base = capi.simple_wave_desc(4, 4, 1, 45.0)
+    dev = torch.ones(4 * 4 * 16, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    swapped = capi.simple_wave_desc(4, 4, 1, 45.0)
+    swapped.tensor_node[0], swapped.tensor_node[1] = 1, 0
+    flat = capi.simple_wave_desc(4, 4, 1, 45.0)
+    flat.area = 0.0
+    for d in (swapped, flat):
+        out = C.c_double(-1.0)
+        assert lib.eg_cell_norm_noalloc(C.byref(d), C.c_void_p(dev.data_ptr()), None, C.byref(out)) == 1
+        assert out.value == -1.0
+    out = C.c_double(-1.0)
+    assert lib.eg_cell_norm_noalloc(C.byref(base), C.c_void_p(dev.data_ptr()), None, C.byref(out)) == capi.OK
+
+
+def test_noalloc_cell_norm_rejects_memory_of_another_device():
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second visible GPU")
+    lib = capi.load()
+    desc = capi.simple_wave_desc(4, 4, 1, 45.0)
+    other = torch.ones(4 * 4 * 16, dtype=torch.float64, device="cuda:1")
+    torch.cuda.synchronize(1)
+    assert lib.eg_set_device(0) == capi.OK
+    out = C.c_double(-1.0)
+    assert lib.eg_cell_norm_noalloc(C.byref(desc), C.c_void_p(other.data_ptr()), None, C.byref(out)) == 1
+    assert out.value == -1.0
