@@ -186,7 +186,7 @@ struct DgOps : LinearOps {
     if (c.opts.precond == EG_PC_BLOCK_ILU0)
       launch_ilu_apply(c, EG_FORM_DG, b, x);
     else
-      launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, b, x);
+      launch_dg_jacobi_apply(c, b, x);
   }
 };
 struct HdgOps : LinearOps {
@@ -870,7 +870,7 @@ int eg_pc_apply(eg_ctx *ctx, const double *b, double *x) {
       if (ilu)
         eg::launch_ilu_apply(c, EG_FORM_DG, c.tmp_body, c.er);
       else
-        eg::launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, c.tmp_body, c.er);
+        eg::launch_dg_jacobi_apply(c, c.tmp_body, c.er);
       c.check_device_error();
       eg::download_vec(c, x, c.er, c.nu);
     } else {

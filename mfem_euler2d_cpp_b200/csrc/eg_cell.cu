@@ -460,6 +460,12 @@ static int sm_count() {
 }
 
 void launch_dg_jacobi(Ctx &c, const double *u, bool factor) {
+  if (factor && dg_inverse_supported(c.q)) {
+    launch_dg_inverse(c, u);
+    c.dg_pc_inverse = true;
+    return;
+  }
+  c.dg_pc_inverse = false;
   c.ensure_pc_dg();
   ProfScope ps(c, EG_K_DG_JACOBI, 1);
   EG_DISPATCH_Q(c.q, {
@@ -472,6 +478,13 @@ void launch_dg_jacobi(Ctx &c, const double *u, bool factor) {
     kern<<<grid, 256, dyn, c.stream>>>(c.geo, c.tab, frozen_of(c), u, c.pc_dg, c.piv_dg, factor, c.derr);
   });
   EG_CUDA(cudaGetLastError());
+}
+
+void launch_dg_jacobi_apply(Ctx &c, const double *b, double *x) {
+  if (c.dg_pc_inverse)
+    launch_dg_inverse_apply(c, b, x);
+  else
+    launch_block_apply(c, c.pc_dg, c.piv_dg, c.n, c.m, b, x);
 }
 
 void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,

@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "eg_cellmat.cuh"
+#include "eg_gj.cuh"
 #include "eg_internal.h"
 
 namespace eg {
@@ -193,33 +194,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// ------------------------------------------- tensor-core Gauss-Jordan
-// D = C + A B on the FP64 tensor pipe: m8n8k4, A row-major 8x4 (one element
-// per lane: row lane/4, column lane%4), B column-major 4x8 (row lane%4,
-// column lane/4), C/D 8x8 (two elements per lane: row lane/4, columns
-// 2*(lane%4) and 2*(lane%4)+1).
-__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-// Reciprocal of a pivot: hardware estimate refined by two Newton-Raphson
-// steps r <- r + r (1 - x r) (quadratic convergence from the ~2^-20 estimate;
-// result within one unit in the last place of 1/x). The estimate flushes
-// subnormal inputs and results to zero, so magnitudes outside
-// [2^-1020, 2^1020] (and zero, infinities, NaN) take IEEE division instead.
-__device__ __forceinline__ double pivot_reciprocal(double x) {
-  const double ax = fabs(x);
-  if (!(ax >= 0x1p-1020 && ax <= 0x1p+1020)) return 1.0 / x;
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  double e = fma(-x, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-x, r, 1.0);
-  return fma(r, e, r);
-}
-
 template <int Q, int WR, int WC>
 struct GjCfg {
   static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1, NC = M + NR;
@@ -230,6 +204,7 @@ struct GjCfg {
   static constexpr int LD = M + 1;           // odd staging stride: conflict-free columns
   static constexpr int KR = (M + 31) / 32;   // rows per lane in the pivot search
 };
+
 
 // Blocked Gauss-Jordan condensation on the tensor cores. The augmented cell
 // system W = [A | B | r_e] lives in registers as 8x8 accumulator tiles; warp
@@ -251,129 +226,6 @@ struct GjCfg {
 // right-hand-side columns hold X_e = A_e^{-1} B_e and y_e = A_e^{-1} r_e,
 // permuted back on the way out (StreamCondense, src/condensation.cpp:136-140,
 // carried to reduced row echelon form: no triangular solve follows).
-// One warp chooses the 4 pivots of a panel staged in `pan` (rows x 4 panel
-// columns) by partial pivoting over the rows not yet used: largest magnitude
-// of the column after eliminating the panel's earlier pivots, first row on
-// ties, NaN never chosen (MFEM LUFactors::Factor). It then publishes T^{-1}
-// of the pivot block (row-major 4x4 in `fac`), the pivot rows (`pivs`) and
-// their unknown indices (`invp`), and turns the pivot rows of the staged A
-// operand into T_r - e_r. Returns false for a zero pivot (singular cell).
-//
-// The search is a dependent chain, so it is kept short: magnitudes are
-// compared as IEEE bit patterns (integer compares, warp max/min reductions),
-// and the column searched at step j+1 is formed fraction-free from the
-// exact values of step j, p (w_{j+1} - (w_j / p) pw_{j+1}) = p w_{j+1} -
-// w_j pw_{j+1}, whose magnitudes order the rows as the eliminated column
-// does (common factor |p|). The exact elimination with multipliers
-// w_j * (1/p), which yields the pivot rows and the multipliers of T's LU
-// factors, runs beside the search instead of in front of it.
-template <int M, int KR>
-__device__ __forceinline__ bool gj_select_pivots(int jbase, double (*pan)[4], double *fac, int *pivs,
-                                                 unsigned char *used, int *invp, int lane) {
-  constexpr unsigned long long kAbs = 0x7fffffffffffffffull, kInf = 0x7ff0000000000000ull;
-  constexpr int kNone = 0x7fffffff;
-  double w[KR][4], key[KR], lm[KR][3];
-  bool un[KR];
-#pragma unroll
-  for (int k = 0; k < KR; ++k) {
-    const int i = lane + 32 * k;
-    un[k] = i < M && !used[i];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) w[k][c] = un[k] ? pan[i][c] : 0.;
-    key[k] = w[k][0];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) lm[k][c] = 0.;
-  }
-  int prow[4];
-  double U[4][4], dinv[4], L[4][4];
-#pragma unroll
-  for (int jj = 0; jj < 4; ++jj) {
-    unsigned long long best = 0ull;
-    int idx = kNone;
-#pragma unroll
-    for (int k = 0; k < KR; ++k) {
-      const unsigned long long bits = (unsigned long long)__double_as_longlong(key[k]) & kAbs;
-      if (un[k] && bits <= kInf && (idx == kNone || bits > best)) {
-        best = bits;
-        idx = lane + 32 * k;
-      }
-    }
-    const unsigned hi = (unsigned)(best >> 32), lo = (unsigned)best;
-    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
-    const bool c1 = idx != kNone && hi == mhi;
-    const unsigned mlo = __reduce_max_sync(0xffffffffu, c1 ? lo : 0u);
-    const bool c2 = c1 && lo == mlo;
-    const int bi = (int)__reduce_min_sync(0xffffffffu, c2 ? (unsigned)idx : (unsigned)kNone);
-    if ((mhi == 0u && mlo == 0u) || bi >= M) return false;
-    prow[jj] = bi;
-    const int owner = bi & 31, kk = bi >> 5;
-    // the pivot row (eliminated by pivots 0..jj-1) and its multipliers
-    double pw[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      double v = 0.;
-#pragma unroll
-      for (int k = 0; k < KR; ++k)
-        if (k == kk) v = w[k][c];
-      pw[c] = c >= jj ? __shfl_sync(0xffffffffu, v, owner) : 0.;
-    }
-#pragma unroll
-    for (int cc = 0; cc < jj; ++cc) {
-      double v = 0.;
-#pragma unroll
-      for (int k = 0; k < KR; ++k)
-        if (k == kk) v = lm[k][cc];
-      L[jj][cc] = __shfl_sync(0xffffffffu, v, owner);
-    }
-#pragma unroll
-    for (int k = 0; k < KR; ++k)
-      if (k == kk && lane == owner) un[k] = false;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) U[jj][c] = pw[c];
-    const double inv = pivot_reciprocal(pw[jj]);
-    dinv[jj] = inv;
-    if (jj < 3) {
-      // the column searched next, fraction-free (no reciprocal on the chain)
-#pragma unroll
-      for (int k = 0; k < KR; ++k) key[k] = fma(pw[jj], w[k][jj + 1], -(w[k][jj] * pw[jj + 1]));
-      // exact elimination of the remaining panel columns
-#pragma unroll
-      for (int k = 0; k < KR; ++k) {
-        const double l = w[k][jj] * inv;
-        lm[k][jj] = l;
-#pragma unroll
-        for (int c = jj + 1; c < 4; ++c) w[k][c] -= l * pw[c];
-      }
-    }
-  }
-  // T^{-1}: lane c < 4 solves T x = e_c with the factors (L, U, 1/pivots)
-  if (lane < 4) {
-    double y[4];
-#pragma unroll
-    for (int rr = 0; rr < 4; ++rr) {
-      double v = rr == lane ? 1. : 0.;
-#pragma unroll
-      for (int cc = 0; cc < rr; ++cc) v -= L[rr][cc] * y[cc];
-      y[rr] = v;
-    }
-#pragma unroll
-    for (int rr = 3; rr >= 0; --rr) {
-      double v = y[rr];
-#pragma unroll
-      for (int cc = rr + 1; cc < 4; ++cc) v -= U[rr][cc] * y[cc];
-      y[rr] = v * dinv[rr];
-    }
-#pragma unroll
-    for (int rr = 0; rr < 4; ++rr) fac[rr * 4 + lane] = y[rr];
-    const int pr = lane == 0 ? prow[0] : lane == 1 ? prow[1] : lane == 2 ? prow[2] : prow[3];
-    pivs[lane] = pr;
-    used[pr] = 1;
-    invp[pr] = jbase + lane;
-    pan[pr][lane] -= 1.;  // A operand T_r - e_r
-  }
-  return true;
-}
-
 template <int Q, int WR, int WC, int MINB>
 __global__ void __launch_bounds__(32 * WR *WC, MINB)
     condense_gj_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,

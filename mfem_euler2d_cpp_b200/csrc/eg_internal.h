@@ -190,8 +190,10 @@ struct Ctx {
   int work_slots = 0;
   double *work_gj = nullptr;    // k >= 5 condensation: one m x (m + 4t + 1) slab per CTA
   int work_gj_slots = 0;
-  // preconditioners (factored in place): DG n blocks m x m, HDG nf blocks t x t
+  // preconditioners (factored in place): DG n blocks m x m, HDG nf blocks t x t;
+  // dg_pc_inverse: pc_dg holds explicit inverses (column-major), else pivoted LU
   double *pc_dg = nullptr, *pc_hdg = nullptr;
+  bool dg_pc_inverse = false;
   int *piv_dg = nullptr, *piv_hdg = nullptr;
   // Krylov workspace (size N = max(nu, nl) so both forms share it)
   int kN = 0, kR = 0;
@@ -257,6 +259,13 @@ void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y);
 void launch_dg_jacobi(Ctx &c, const double *u, bool factor);
 void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,
                         const double *b, double *x);
+// DG block-Jacobi apply x = J_KK^{-1} b with whichever factors the last
+// launch_dg_jacobi(factor = true) formed (explicit inverses or pivoted LU).
+void launch_dg_jacobi_apply(Ctx &c, const double *b, double *x);
+// ---- explicit DG block-Jacobi inverses (eg_dginv.cu) ----
+bool dg_inverse_supported(int q);
+void launch_dg_inverse(Ctx &c, const double *u);  // pc_dg <- column-major J_KK^{-1}
+void launch_dg_inverse_apply(Ctx &c, const double *b, double *x);
 // ---- launchers (eg_hdg.cu) ----
 void launch_condense(Ctx &c, const double *u, const double *r);
 void launch_schur_apply(Ctx &c, const double *v, double *y);

@@ -12,8 +12,13 @@
 #include "euler.hpp"
 
 #include <algorithm>
+#include <array>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
+#include <string>
+#include <vector>
 
 using namespace euler;
 
@@ -311,5 +316,174 @@ int ref_ilu(void *hv, int form, const double *u, const double *b, double *x, dou
 // Switch the preconditioner of an existing handle (0 block-jacobi, 1 block-ilu0).
 void ref_set_precond(void *hv, int precond) {
   static_cast<RefHandle *>(hv)->opt.precond = precond ? "block-ilu0" : "block-jacobi";
+}
+
+// Per-update trajectory of the reference time loop. The options come from the
+// reference's own parser (ParseOptions, src/options.cpp:8) on the command-line
+// arguments argv[0..argc), so the run is the one the euler2d command line
+// makes. The loop restates euler::Run (src/stepper.cpp:28-252) step for step
+// on the reference's Problem, LinearSolver, StreamCondense and Recover, with
+// the timers, CSV output and --check-update left out, and records for every
+// accepted Newton update (in order) the Newton direction du (the recovered
+// body update for HDG, stepper.cpp:163; the DG solve's x, :145) and the
+// line-search damping (:204-217). u_final receives the final state, which the
+// fixture generator requires to equal the command line's final coefficients.
+int ref_trajectory(int argc, const char **argv, int hdg_form, int max_updates, double *du_out,
+                   double *damping_out, double *u_final, int *count) {
+  return guarded([&] {
+    std::vector<char *> av(argc + 1);
+    std::vector<std::string> store(argv, argv + argc);
+    std::string prog = "euler2d";
+    av[0] = prog.data();
+    for (int i = 0; i < argc; ++i) av[i + 1] = store[i].data();
+    Options o = ParseOptions(argc + 1, av.data());
+    const EulerGas gas(3.);
+    Problem p(o, gas);
+    const std::string form = hdg_form ? "hdg" : "dg";
+    Vector u = p.Initial();
+    require(p.Admissible(u), "Initial projection not positive; refine mesh");
+    Vector residual(p.nu), rhs(p.nu), er(p.nu), du(p.nu), trial(p.nu), trial_residual(p.nu),
+        step_state(p.nu), stage_base(p.nu);
+    std::array<Vector, 4> slope;
+    for (auto &v : slope) v.SetSize(p.nu);
+    Hybrid hybrid;
+    Condensed condensed;
+    if (hdg_form) p.PrepareHybrid(hybrid, condensed);
+    std::unique_ptr<ElementOperator> dg_jacobian;
+    if (!hdg_form && o.assembly == "partial") dg_jacobian = p.PartialDG(u, false);
+    const int global_size = hdg_form ? p.nl : p.nu;
+    LinearSolver linear_solver(global_size, hdg_form ? p.t : p.m, o, hdg_form ? p.trace_metric : p.cell_metric);
+    if (o.solver == "gmres" && o.precond == "block-ilu0") linear_solver.Prepare(p.SolverGraph(hdg_form != 0), o);
+    LinearResult lr, attempt;
+    lr.x.SetSize(global_size);
+    lr.equation_residual.SetSize(global_size);
+    attempt.x.SetSize(global_size);
+    attempt.equation_residual.SetSize(global_size);
+    Options linear = o;
+    constexpr double alpha = 0.24169426078821, beta = alpha / 4., eta = 0.12915286960590;
+    const double A[4][4] = {{alpha, 0., 0., 0.},
+                            {-alpha, alpha, 0., 0.},
+                            {0., 1. - alpha, alpha, 0.},
+                            {beta, eta, .5 - beta - eta - alpha, alpha}};
+    const double b[4] = {0., 1. / 6., 1. / 6., 2. / 3.};
+    double time = 0.;
+    int step = 0, n_upd = 0;
+    bool final_step = time >= o.end;
+    while (o.steps > 0 ? step < o.steps : !final_step) {
+      step_state = u;
+      p.Freeze(step_state, o.dt, false);
+      const double rate = p.WaveRate();
+      double dt = o.cfl > 0 ? o.cfl / rate : o.dt;
+      if (o.steps < 0) {
+        final_step = time + dt >= o.end;
+        if (final_step) dt = o.end - time;
+      }
+      require(std::isfinite(dt) && dt > 0 && time + dt < 4 / ((p.gas.Gamma() + 1) * pi),
+              "Step leaves the smooth simple-wave interval T < 4/((gamma+1)*pi)");
+      const int stages = o.integrator == "be" ? 1 : 4;
+      for (int stage = 0; stage < stages; ++stage) {
+        const double diagonal = o.integrator == "be" ? 1. : A[stage][stage];
+        stage_base = step_state;
+        if (o.integrator != "be")
+          for (int j = 0; j < stage; ++j) stage_base.Add(dt * A[stage][j], slope[j]);
+        if (stage > 0) p.Freeze(u, diagonal * dt, false);
+        p.dt = diagonal * dt;
+        p.old = stage_base;
+        const double physical_scale = 1 / (p.dt * std::sqrt(p.lx * p.ly));
+        const double old_norm = p.CellNorm(stage_base);
+        double r0 = -1.;
+        bool converged = false, residual_ready = false;
+        const int limit = o.newton_steps > 0 ? o.newton_steps : o.max_newton;
+        for (int it = 0; it <= limit; ++it) {
+          if (!residual_ready) p.Residual(u, residual);
+          const double residual_norm = p.CellNorm(residual);
+          const double rms = physical_scale * residual_norm;
+          if (r0 < 0) r0 = rms;
+          if (o.newton_steps < 0 && rms <= o.tol * std::max(1., r0)) {
+            converged = true;
+            break;
+          }
+          if (it == limit) break;
+          double er_norm = 0.;
+          lr.count = 0;
+          const double allowance = 128 * std::numeric_limits<double>::epsilon() *
+                                   (p.CellNorm(u) + old_norm + residual_norm);
+          const double target = std::max(10 * o.linear_tol * residual_norm, allowance);
+          if (!hdg_form) {
+            if (o.assembly == "partial") dg_jacobian->Refresh(u);
+            else dg_jacobian = p.DG(u);
+            rhs = residual;
+            rhs *= -1;
+            linear_solver.Solve(*dg_jacobian, rhs, o, lr);
+            du = lr.x;
+            er_norm = p.CellNorm(lr.equation_residual);
+          } else {
+            auto &h = hybrid;
+            auto &s = condensed;
+            p.StreamCondense(u, residual, h, s);
+            linear.linear_tol = o.linear_tol;
+            bool valid = false;
+            for (int a = 0; a < 4; ++a) {
+              linear_solver.Solve(*s.op, s.rhs, linear, attempt, a == 0);
+              p.Recover(s, attempt.x, du);
+              // RecoveredResidual (src/stepper.cpp:10-26): er = -B (eps_S / D)
+              auto &scaled = s.scaled_scratch;
+              for (int f = 0; f < p.nf; ++f)
+                for (int i = 0; i < p.t; ++i) scaled[f * p.t + i] = attempt.equation_residual[f * p.t + i] / h.D[f * p.t + i];
+              auto &local = s.local_scratch;
+              auto &cell = s.cell_scratch;
+              for (int e = 0; e < p.n; ++e) {
+                for (int i = 0; i < 4 * p.t; ++i) local[i] = scaled[h.ids[e][i]];
+                h.B[e].Mult(local, cell);
+                for (int i = 0; i < p.m; ++i) er[e * p.m + i] = -cell[i];
+              }
+              er_norm = p.CellNorm(er);
+              valid = er_norm <= target;
+              if (valid) break;
+              require(o.solver == "gmres", "Direct Schur solve fails DG residual criterion");
+              linear.linear_tol *= .01;
+            }
+            require(valid, "Recovered DG residual criterion failed after Schur refinement");
+          }
+          require(er_norm <= target, "DG Newton linear residual too large");
+          double damping = 1.;
+          bool accept = false;
+          for (int back = 0; back < 30; ++back) {
+            trial = u;
+            trial.Add(damping, du);
+            if (p.Admissible(trial)) {
+              p.Residual(trial, trial_residual);
+              if (p.CellNorm(trial_residual) <= (1 - 1e-4 * damping) * residual_norm + allowance) {
+                accept = true;
+                break;
+              }
+            }
+            damping *= .5;
+          }
+          require(accept, "Newton line search failed");
+          require(n_upd < max_updates, "trajectory buffer too small");
+          std::memcpy(du_out + (size_t)n_upd * p.nu, du.GetData(), sizeof(double) * p.nu);
+          damping_out[n_upd] = damping;
+          ++n_upd;
+          u = trial;
+          residual = trial_residual;
+          residual_ready = true;
+        }
+        require(converged || o.newton_steps > 0, "Newton failed to converge");
+        slope[stage] = u;
+        slope[stage] -= stage_base;
+        slope[stage] *= 1. / p.dt;
+      }
+      if (o.integrator != "be") {
+        u = step_state;
+        for (int stage = 0; stage < 4; ++stage) u.Add(dt * b[stage], slope[stage]);
+        require(p.Admissible(u), "SSP-DIRK3 step produced an inadmissible state");
+      }
+      time = o.steps < 0 && final_step ? o.end : time + dt;
+      ++step;
+    }
+    std::memcpy(u_final, u.GetData(), sizeof(double) * p.nu);
+    *count = n_upd;
+  });
 }
 }

@@ -14,7 +14,20 @@ compiled against the MFEM-subset shim. Two kinds of fixture are written:
   full assembly: final coefficients per form and the per-update
   _iterations.csv columns.
 
-Usage:  python tests/golden/make_golden.py [--only CLI_CASE ...]
+* traj_*.npz   -- every accepted Newton update of a command-line case: the
+  Newton direction du (the recovered body update for HDG) and the damping,
+  from the reference's time loop on its own objects (ref_trajectory), whose
+  final state must equal the command line's.
+
+* condense_*.npz -- condensation, Schur action and recovery at k = 5..8 on
+  meshes with more cells than the device condensation has CTAs.
+
+* c2_*.npz     -- the reference command line on the 128x128 Q4 workload (HDG
+  with block Jacobi and block ILU(0), DG with block Jacobi): every
+  _iterations.csv row, the summary and a strided sample of the final state.
+
+Usage:  python tests/golden/make_golden.py
+            [--only CLI_CASE ... | --trajectories | --condense | --c2 [CASE ...]]
 """
 from __future__ import annotations
 
@@ -72,6 +85,7 @@ def load_ref():
     lib.ref_linear_solve.argtypes = [C.c_void_p, C.c_int, DP, DP, DP, DP, IP, DP]
     lib.ref_ilu.argtypes = [C.c_void_p, C.c_int, DP, DP, DP, DP, DP, IP]
     lib.ref_set_precond.argtypes = [C.c_void_p, C.c_int]
+    lib.ref_trajectory.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_int, C.c_int, DP, DP, DP, IP]
     return lib
 
 
@@ -277,11 +291,157 @@ def make_cli(exe: Path, name: str, args: list[str]) -> dict:
         return out
 
 
+# (nx, ny, k, alpha_deg): high degrees on meshes with more cells than the
+# condensation launches CTAs (two per SM for k = 5, 6 and one for k = 7, 8 on
+# 148 SMs), so that CTAs reduce several cells each (condense_*.npz)
+CONDENSE_CASES = [(18, 18, 5, 33.0), (18, 18, 6, 47.0), (13, 13, 7, 58.0), (13, 13, 8, 26.0)]
+
+
+def make_condense(lib, nx, ny, k, alpha, seed):
+    """Condensed HDG pieces at a perturbed state: StreamCondense's rhs, y and
+    D, the Schur action on a seeded vector and the recovery of another
+    (condensation.cpp:131-163, operators.cpp:147). The vectors v and lam are
+    regenerated from `seed` by numpy.random.default_rng; old is the initial
+    projection."""
+    h = lib.ref_problem_new(nx, ny, k, alpha, 1.1, 0, 0, 20, 1500, 1e-12)
+    if not h:
+        raise RuntimeError(lib.ref_last_error().decode())
+    try:
+        sz = np.zeros(7, np.int32)
+        lib.ref_sizes(h, sz.ctypes.data_as(IP))
+        n, p, m, t, nf, nu, nl = map(int, sz)
+        geo = np.zeros(5)
+        lib.ref_geometry(h, ptr(geo))
+        u0 = np.zeros(nu)
+        check(lib, lib.ref_initial(h, ptr(u0)))
+        rng = np.random.default_rng(seed)
+        u = u0 * np.repeat(1.0 + 0.01 * np.sin(0.37 * np.arange(nu // 4) + 0.3), 4)
+        u = u + 1e-5 * rng.standard_normal(nu) * np.abs(u)
+        if not lib.ref_admissible(h, ptr(u)):
+            raise RuntimeError("perturbed state not admissible")
+        dt = 0.05 * min(geo[2], geo[3])
+        a, b, rate = np.zeros(nf * (k + 1)), np.zeros(nf * (k + 1)), np.zeros(1)
+        check(lib, lib.ref_freeze(h, ptr(u), dt, 1, ptr(a), ptr(b), ptr(rate)))
+        check(lib, lib.ref_set_old(h, ptr(u0)))
+        lib.ref_set_dt(h, dt)
+        r = np.zeros(nu)
+        check(lib, lib.ref_residual(h, ptr(u), ptr(r)))
+        rhs, X, y, D = np.zeros(nl), np.zeros(n * m * 4 * t), np.zeros(nu), np.zeros(nl)
+        check(lib, lib.ref_hdg_condense(h, ptr(u), ptr(r), ptr(rhs), ptr(X), ptr(y), ptr(D)))
+        vrng = np.random.default_rng([seed, 1])
+        v, lam = vrng.standard_normal(nl), vrng.standard_normal(nl)
+        sv, du = np.zeros(nl), np.zeros(nu)
+        check(lib, lib.ref_schur_apply(h, ptr(v), ptr(sv)))
+        check(lib, lib.ref_recover(h, ptr(lam), ptr(du)))
+        return dict(nx=nx, ny=ny, k=k, alpha=alpha, dt=dt, seed=seed, u=u, rhs=rhs, y_hdg=y, D=D, sv=sv, du=du)
+    finally:
+        lib.ref_problem_free(h)
+
+
+# The headline 128x128 Q4 workload (5 SSP-DIRK3 steps x 3 Newton updates per
+# stage), one form and preconditioner per case. Its final states are 13 MB
+# each, so the fixture keeps every _iterations.csv row, the summary row, the
+# per-component sums of squares of the final state and every STRIDE-th
+# coefficient of it (c2_*.npz).
+C2_ARGS = ["--nx", "128", "--ny", "128", "--k", "4", "--alpha-deg", "30", "--cfl", "1", "--steps", "5",
+           "--newton-steps", "3", "--assembly", "partial"]
+C2_CASES = {
+    "hdg_jacobi": ["--form", "hdg", "--precond", "block-jacobi"],
+    "hdg_ilu0": ["--form", "hdg", "--precond", "block-ilu0"],
+    "dg_jacobi": ["--form", "dg", "--precond", "block-jacobi"],
+}
+C2_STRIDE = 32
+
+
+def make_c2(exe: Path, names: list[str]) -> None:
+    """Run the reference command line on the c2 cases in parallel (one
+    process each) and write c2_<name>.npz."""
+    with tempfile.TemporaryDirectory() as tmp:
+        procs = {}
+        for name in names:
+            prefix = Path(tmp) / name
+            args = C2_ARGS + C2_CASES[name]
+            procs[name] = (args, prefix, subprocess.Popen([str(exe), *args, "--output", str(prefix)],
+                                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                                          text=True))
+        for name, (args, prefix, proc) in procs.items():
+            _, err = proc.communicate()
+            if proc.returncode:
+                raise RuntimeError(f"c2 {name}: {err}")
+            form = args[args.index("--form") + 1]
+            coeff = np.loadtxt(f"{prefix}_{form}_coefficients.csv", delimiter=",", skiprows=1)
+            u = coeff[:, 2:].reshape(-1)
+            with open(f"{prefix}_{form}_iterations.csv", newline="") as fh:
+                rows = list(csv.DictReader(fh))
+            with open(f"{prefix}_{form}_summary.csv", newline="") as fh:
+                summ = next(csv.DictReader(fh))
+            out = {"args": np.array(json.dumps(args)), "stride": np.array([C2_STRIDE]),
+                   "iterations": np.array([[float(r[c]) for c in ITER_COLS] for r in rows]),
+                   "summary": np.array([float(summ[c]) for c in SUMMARY_COLS]),
+                   "u_sample": u[::C2_STRIDE].copy(), "u_size": np.array([u.size]),
+                   "u_component_sumsq": (u.reshape(-1, 4) ** 2).sum(axis=0),
+                   "mean_newton_s": np.array([float(summ["mean_newton_s"])])}
+            np.savez_compressed(HERE / f"c2_{name}.npz", **out)
+            print("c2", name, len(rows), "updates")
+
+
+# command-line cases whose every Newton update is recorded (traj_*.npz)
+TRAJ_CASES = ["c1_16x16_q3"]
+
+
+def make_trajectory(lib, name: str) -> dict:
+    """Newton direction du and damping of every accepted update of both forms
+    (oracle/ref_harness.cpp ref_trajectory), pinned to the command line: the
+    trajectory's final state must equal the cli_<name>.npz final state."""
+    args = CLI_CASES[name]
+    argv = (C.c_char_p * len(args))(*[a.encode() for a in args])
+    cli = np.load(HERE / f"cli_{name}.npz")
+    u0 = cli["u0"]
+    nu = u0.size
+    out = {"args": np.array(json.dumps(args))}
+    for hdg, tag in ((0, "dg"), (1, "hdg")):
+        cap = 4096
+        du = np.zeros(cap * nu)
+        damping = np.zeros(cap)
+        u_final = np.zeros(nu)
+        cnt = np.zeros(1, np.int32)
+        check(lib, lib.ref_trajectory(len(args), argv, hdg, cap, ptr(du), ptr(damping), ptr(u_final),
+                                      cnt.ctypes.data_as(IP)))
+        n = int(cnt[0])
+        ref_u = cli[f"{tag}_u"]
+        err = np.linalg.norm(u_final - ref_u) / np.linalg.norm(ref_u)
+        # the command-line fixture may come from the AVX-512 build and the
+        # harness library from the AVX2 one: vectorisation changes rounding only
+        if err > 1e-13:
+            raise RuntimeError(f"{name} {tag}: trajectory final state differs from the command line ({err:.3e})")
+        out[f"{tag}_final_vs_cli"] = np.array([err])
+        if n != len(cli[f"{tag}_iterations"]):
+            raise RuntimeError(f"{name} {tag}: {n} updates against {len(cli[f'{tag}_iterations'])} CSV rows")
+        out[f"{tag}_du"] = du[: n * nu].reshape(n, nu)
+        out[f"{tag}_damping"] = damping[:n]
+    return out
+
+
 def main():
     if not (REF / "libeuler_ref.so").exists():
         sys.exit("oracle/_ref is not built: run `make -C oracle` where the reference is available")
     lib = load_ref()
     only = sys.argv[sys.argv.index("--only") + 1:] if "--only" in sys.argv else None
+    if "--c2" in sys.argv:  # the 128x128 Q4 cases (several CPU minutes each, run in parallel)
+        names = sys.argv[sys.argv.index("--c2") + 1:] or list(C2_CASES)
+        make_c2(ref_cli(), names)
+        return
+    if "--condense" in sys.argv:  # regenerate just the high-degree condensation cases
+        for i, (nx, ny, k, alpha) in enumerate(CONDENSE_CASES):
+            np.savez_compressed(HERE / f"condense_{nx}x{ny}_k{k}.npz",
+                                **make_condense(lib, nx, ny, k, alpha, 7000 + i))
+            print("condense", nx, ny, k)
+        return
+    if "--trajectories" in sys.argv:  # regenerate just the per-update trajectories
+        for name in TRAJ_CASES:
+            np.savez_compressed(HERE / f"traj_{name}.npz", **make_trajectory(lib, name))
+            print("trajectory", name)
+        return
     if only:  # regenerate just the named command-line cases (and the manifest)
         exe = ref_cli()
         for name in only:
@@ -304,6 +464,12 @@ def main():
         data["u0"] = ref_initial_state(lib, args)
         np.savez_compressed(HERE / f"cli_{name}.npz", **data)
         print("cli", name)
+    for name in TRAJ_CASES:
+        np.savez_compressed(HERE / f"traj_{name}.npz", **make_trajectory(lib, name))
+        print("trajectory", name)
+    for i, (nx, ny, k, alpha) in enumerate(CONDENSE_CASES):
+        np.savez_compressed(HERE / f"condense_{nx}x{ny}_k{k}.npz", **make_condense(lib, nx, ny, k, alpha, 7000 + i))
+        print("condense", nx, ny, k)
     meta = {"iteration_columns": ITER_COLS, "summary_columns": SUMMARY_COLS,
             "unit_cases": UNIT_CASES, "cli_cases": CLI_CASES}
     (HERE / "manifest.json").write_text(json.dumps(meta, indent=1))

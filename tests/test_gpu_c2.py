@@ -1,0 +1,65 @@
+"""Parity at the benchmarked 128x128 Q4 workload (SSP-DIRK3, CFL 1, 5 steps x
+3 Newton updates per stage): the euler2d --device cuda command line against
+the reference command line's own run (tests/golden/c2_*.npz), update by
+update, for HDG with block Jacobi and block ILU(0) and for DG with block
+Jacobi.
+
+Per update (every _iterations.csv row): step/stage/newton indices and the
+line-search damping identical, the physical residual rms within 1e-8
+relative, dt within 1e-12, Krylov counts within two iterations. Final state:
+every 32nd coefficient within 1e-10 relative and the per-component sums of
+squares within 1e-10; L2 errors within 1e-9 relative; conservation drift
+below 1e-13 as the reference's.
+"""
+import csv
+import json
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, manifest, rel_err
+
+pytestmark = pytest.mark.gpu
+CLI = ROOT / "mfem_euler2d_cpp_b200" / "bin" / "euler2d"
+CASES = sorted(GOLDEN.glob("c2_*.npz"))
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.stem)
+def test_headline_workload_update_by_update(path, tmp_path):
+    f = np.load(path)
+    args = json.loads(str(f["args"]))
+    form = args[args.index("--form") + 1]
+    prefix = tmp_path / "run"
+    proc = subprocess.run([str(CLI), *args, "--output", str(prefix)], capture_output=True, text=True, timeout=900)
+    assert proc.returncode == 0, proc.stderr
+    meta = manifest()
+    icol, scol = meta["iteration_columns"], meta["summary_columns"]
+    c = {name: i for i, name in enumerate(icol)}
+    with open(f"{prefix}_{form}_iterations.csv", newline="") as fh:
+        iters = np.array([[float(r[name]) for name in icol] for r in csv.DictReader(fh)])
+    ref = f["iterations"]
+    assert iters.shape == ref.shape
+    for name in ("step", "stage", "newton"):
+        np.testing.assert_array_equal(iters[:, c[name]], ref[:, c[name]])
+    np.testing.assert_array_equal(iters[:, c["damping"]], ref[:, c["damping"]])
+    rms, ref_rms = iters[:, c["residual_physical_rms"]], ref[:, c["residual_physical_rms"]]
+    assert np.max(np.abs(rms - ref_rms) / np.abs(ref_rms)) < 1e-8
+    assert np.max(np.abs(iters[:, c["dt"]] - ref[:, c["dt"]]) / ref[:, c["dt"]]) < 1e-12
+    assert np.all(np.abs(iters[:, c["krylov_iterations"]] - ref[:, c["krylov_iterations"]]) <= 2)
+    coeff = np.loadtxt(f"{prefix}_{form}_coefficients.csv", delimiter=",", skiprows=1)
+    u = coeff[:, 2:].reshape(-1)
+    assert u.size == int(f["u_size"][0])
+    stride = int(f["stride"][0])
+    assert rel_err(u[::stride], f["u_sample"]) < 1e-10
+    sumsq = (u.reshape(-1, 4) ** 2).sum(axis=0)
+    assert np.max(np.abs(sumsq - f["u_component_sumsq"]) / f["u_component_sumsq"]) < 1e-10
+    with open(f"{prefix}_{form}_summary.csv", newline="") as fh:
+        summary = next(csv.DictReader(fh))
+    s = {name: float(summary[name]) for name in scol}
+    rs = dict(zip(scol, f["summary"]))
+    assert s["newton_updates"] == rs["newton_updates"]
+    assert s["time_steps"] == rs["time_steps"]
+    for name in ("rho_L2", "rhou_L2", "rhov_L2", "energy_L2"):
+        assert abs(s[name] - rs[name]) <= 1e-9 * rs[name] + 1e-15
+    assert s["max_conservation_drift"] < 1e-13

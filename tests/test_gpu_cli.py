@@ -65,7 +65,7 @@ def test_cli_matches_reference(path, tmp_path):
         assert abs(s["T"] - rs["T"]) <= 1e-14 * max(1, abs(rs["T"]))
         for name in ("rho_L2", "rhou_L2", "rhov_L2", "energy_L2"):
             assert abs(s[name] - rs[name]) <= 1e-9 * rs[name] + 1e-15
-        assert s["max_conservation_drift"] < 1e-12
+        assert s["max_conservation_drift"] < 1e-13  # the reference's own drift here: 3e-15 to 3.4e-14
         assert summary["device"] == "cuda"
         assembly = args[args.index("--assembly") + 1] if "--assembly" in args else "partial"
         assert summary["assembly"] == assembly

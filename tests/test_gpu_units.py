@@ -9,7 +9,7 @@ to 1e-10 relative, with Krylov counts within one iteration of the reference.
 import numpy as np
 import pytest
 
-from conftest import rel_err, unit_files
+from conftest import GOLDEN, rel_err, unit_files
 from mfem_euler2d_cpp_b200 import capi
 
 pytestmark = pytest.mark.gpu
@@ -225,3 +225,36 @@ def test_pivot_reciprocal_within_one_ulp_of_division():
     assert np.all(np.abs(y[finite] - ref[finite]) <= ulp)
     # overflow to infinity and results below the normal range match division exactly
     assert np.array_equal(y[~finite], ref[~finite])
+
+
+@pytest.fixture(params=sorted(GOLDEN.glob("condense_*.npz")), ids=lambda p: p.stem)
+def condense_case(request):
+    return np.load(request.param)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_high_degree_condensation_on_many_cells(condense_case, precision):
+    """k = 5..8 on meshes with more cells than the condensation launches CTAs
+    (each CTA reduces several cells in its slab): D, the Schur right-hand
+    side, y, the Schur action and the recovery against the reference. The
+    mixed-precision context condenses in FP64 too, so it meets the same bar."""
+    f = condense_case
+    nx, ny, k = int(f["nx"]), int(f["ny"]), int(f["k"])
+    d = capi.simple_wave_desc(nx, ny, k, float(f["alpha"]))
+    prec = capi.PRECISION_MIXED if precision == "mixed" else capi.PRECISION_FP64
+    with capi.Context(d, capi.default_opts(form=capi.FORM_HDG, precision=prec)) as ctx:
+        ctx.initial()
+        u0 = ctx.download("U")
+        ctx.upload("U", f["u"])
+        ctx.freeze(float(f["dt"]), check_admissible=True)
+        ctx.upload("OLD", u0)
+        ctx.set_dt(float(f["dt"]))
+        ctx.residual()
+        ctx.condense()
+        assert rel_err(ctx.download("D"), f["D"]) < OP_TOL
+        assert rel_err(ctx.download("RHS"), f["rhs"]) < OP_TOL
+        assert rel_err(ctx.download("Y"), f["y_hdg"]) < OP_TOL
+        vrng = np.random.default_rng([int(f["seed"]), 1])
+        v, lam = vrng.standard_normal(ctx.nl), vrng.standard_normal(ctx.nl)
+        assert rel_err(ctx.schur_apply(v), f["sv"]) < OP_TOL
+        assert rel_err(ctx.recover(lam), f["du"]) < OP_TOL
