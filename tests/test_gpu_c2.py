@@ -9,7 +9,9 @@ line-search damping identical, the physical residual rms within 1e-8
 relative, dt within 1e-12, Krylov counts within two iterations. Final state:
 every 32nd coefficient within 1e-10 relative and the per-component sums of
 squares within 1e-10; L2 errors within 1e-9 relative; conservation drift
-below 1e-13 as the reference's.
+within 1e-13 of the reference's own (1.12e-12 here: with three Newton updates
+per stage the stage residuals stay near 1e-8, so neither code conserves to
+roundoff on this workload).
 """
 import csv
 import json
@@ -62,4 +64,4 @@ def test_headline_workload_update_by_update(path, tmp_path):
     assert s["time_steps"] == rs["time_steps"]
     for name in ("rho_L2", "rhou_L2", "rhov_L2", "energy_L2"):
         assert abs(s[name] - rs[name]) <= 1e-9 * rs[name] + 1e-15
-    assert s["max_conservation_drift"] < 1e-13
+    assert abs(s["max_conservation_drift"] - rs["max_conservation_drift"]) <= 1e-13
