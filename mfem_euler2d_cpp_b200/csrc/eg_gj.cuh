@@ -163,4 +163,128 @@ __device__ __forceinline__ bool gj_select_pivots(int jbase, double (*pan)[4], do
 }
 
 
+// ------------------------------------ two-phase Gauss-Jordan (A in smem)
+// One warp chooses the 4 pivots of the panel whose columns are Acol[c*LDA+i]
+// (c < 4, column-major, rows i < M) among the rows not yet used, by row
+// partial pivoting: the row of largest magnitude in the column after the
+// panel's earlier pivots are eliminated (MFEM LUFactors::Factor). The search
+// runs fraction-free: the column searched at step s is p w - w_s pw over the
+// previous step's values (scaled by the earlier pivots, which orders the rows
+// as the eliminated column does), so no reciprocal sits on the chain. One
+// warp max-reduction per step on a packed key (25 magnitude bits of the
+// IEEE pattern and 127 - row, so ties go to the first row; magnitudes within
+// 2^-13 of each other count as ties, a choice as stable as the exact one);
+// the pivot row reaches every lane through shared memory (rowbuf). Writes the
+// pivot rows (pivs), marks them used and records their unknown index (invp);
+// returns false for a zero column (singular cell; the remaining pivots are
+// the first unused rows, so the caller's loop stays well defined).
+template <int M, int KR, int LDA>
+__device__ __forceinline__ bool gj_pick_pivots(int jbase, const double *Acol, double (*rowbuf)[4], int *pivs,
+                                               unsigned char *used, int *invp, int lane) {
+  double w[KR][4];
+  bool un[KR];
+#pragma unroll
+  for (int k = 0; k < KR; ++k) {
+    const int i = lane + 32 * k;
+    un[k] = i < M && !used[i];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) w[k][c] = un[k] ? Acol[c * LDA + i] : 0.;
+  }
+  int prow[4];
+  bool ok = true;
+#pragma unroll
+  for (int jj = 0; jj < 4; ++jj) {
+    unsigned best = 0u;
+#pragma unroll
+    for (int k = 0; k < KR; ++k) {
+      const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(w[k][jj]) >> 32) & 0x7fffffffu;
+      const unsigned pk =
+          (un[k] && hi <= 0x7ff00000u) ? (((hi >> 7) << 7) | (unsigned)(127 - (lane + 32 * k))) : 0u;
+      best = pk > best ? pk : best;
+    }
+    const unsigned mb = __reduce_max_sync(0xffffffffu, best);
+    int bi = 127 - (int)(mb & 127u);
+    if ((mb >> 7) == 0u) {
+      ok = false;
+      int cand = 0x7fffffff;
+#pragma unroll
+      for (int k = KR - 1; k >= 0; --k)
+        if (un[k]) cand = lane + 32 * k;
+      bi = (int)__reduce_min_sync(0xffffffffu, (unsigned)cand);
+    }
+    prow[jj] = bi;
+    if (jj < 3) {
+      __syncwarp();
+      double pw[4];
+#pragma unroll
+      for (int c = jj; c < 4; ++c) pw[c] = jj == 0 ? Acol[c * LDA + bi] : rowbuf[bi][c];
+#pragma unroll
+      for (int k = 0; k < KR; ++k) {
+        const int i = lane + 32 * k;
+        if (i == bi) un[k] = false;
+#pragma unroll
+        for (int c = jj + 1; c < 4; ++c) w[k][c] = fma(pw[jj], w[k][c], -(w[k][jj] * pw[c]));
+        if (un[k]) {
+#pragma unroll
+          for (int c = jj + 1; c < 4; ++c) rowbuf[i][c] = w[k][c];
+        }
+      }
+    }
+  }
+  if (lane < 4) {
+    const int pr = lane == 0 ? prow[0] : lane == 1 ? prow[1] : lane == 2 ? prow[2] : prow[3];
+    pivs[lane] = pr;
+    used[pr] = 1;
+    invp[pr] = jbase + lane;
+  }
+  return ok;
+}
+
+// T^{-1} (row-major 4x4 in fac) of the pivot block T[r][c] = Acol[c*LDA +
+// pivs[r]], by lanes 0..3 of one warp: LU of T in pivot order (no further
+// pivoting: the rows were chosen by partial pivoting), then lane c solves
+// T x = e_c. Afterwards the pivot rows of the panel hold T_r - e_r, the A
+// operand that turns the update of a pivot row into its normalisation.
+template <int LDA>
+__device__ __forceinline__ void gj_pivot_block_inverse(double *Acol, const int *pivs, double *fac, int lane) {
+  if (lane < 4) {
+    double T[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) T[r][c] = Acol[c * LDA + pivs[r]];
+    double dinv[4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      dinv[kk] = pivot_reciprocal(T[kk][kk]);
+#pragma unroll
+      for (int r = kk + 1; r < 4; ++r) {
+        const double l = T[r][kk] * dinv[kk];
+        T[r][kk] = l;
+#pragma unroll
+        for (int c = kk + 1; c < 4; ++c) T[r][c] = fma(-l, T[kk][c], T[r][c]);
+      }
+    }
+    double y[4];
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) {
+      double v = rr == lane ? 1. : 0.;
+#pragma unroll
+      for (int cc = 0; cc < rr; ++cc) v = fma(-T[rr][cc], y[cc], v);
+      y[rr] = v;
+    }
+#pragma unroll
+    for (int rr = 3; rr >= 0; --rr) {
+      double v = y[rr];
+#pragma unroll
+      for (int cc = 3; cc > rr; --cc) v = fma(-T[rr][cc], y[cc], v);
+      y[rr] = v * dinv[rr];
+    }
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) fac[rr * 4 + lane] = y[rr];
+  }
+  __syncwarp();
+  if (lane < 4) Acol[lane * LDA + pivs[lane]] -= 1.;
+}
+
 }  // namespace eg

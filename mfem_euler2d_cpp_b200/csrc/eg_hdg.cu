@@ -47,11 +47,13 @@ struct CondenseShared {
 };
 
 // Assemble the cell system: A (m x m) and [B | r_e] (m x (4t+1)), both
-// column-major with leading dimension m; also store C and the B scalars.
+// column-major, A with leading dimension ld and [B | r_e] with ldr (ld when
+// not given); also store C and the B scalars.
 template <int Q>
 __device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen &fz,
                                const double *__restrict__ u, const double *__restrict__ r, double *Cb,
-                               double *sf_out, double *A, double *R, int e, int ld = 4 * Q * Q) {
+                               double *sf_out, double *A, double *R, int e, int ld = 4 * Q * Q, int ldr = -1) {
+  if (ldr < 0) ldr = ld;
   constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
   const STab<Q> &st = sh.st;
   for (int i = threadIdx.x; i < M; i += blockDim.x) sh.us[i] = u[(size_t)e * M + i];
@@ -99,7 +101,7 @@ __device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen
   __syncthreads();
   build_cell_matrix<Q>(A, ld, st, sh.us, sh.FM, g);
   for (int col = threadIdx.x; col < NR; col += blockDim.x) {
-    double *rc = R + (size_t)col * ld;
+    double *rc = R + (size_t)col * ldr;
     if (col < 4 * T) {
       for (int i = 0; i < M; ++i) rc[i] = 0.;
       const int s = col / T, jj = (col % T) >> 2, c = col & 3;
@@ -357,6 +359,211 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
           const int col = (wc + b * WC) * 8 + 2 * tq;
           if (col >= M && col < NC) R[(size_t)(col - M) * M + jrow] = acc[a][b][0];
           if (col + 1 >= M && col + 1 < NC) R[(size_t)(col + 1 - M) * M + jrow] = acc[a][b][1];
+        }
+      }
+    }
+    __syncthreads();
+    condense_epilogue<Q>(sh, R, true, XY, contrib, panels, g.npan, e);
+  }
+}
+
+// ------------------------------------- two-phase condensation (k <= 4)
+// The cell system [A | B | r_e] of the register-resident kernel above fills
+// an SM's register file, so one cell's serial pivot chain leaves the SM idle
+// most of the time. This kernel splits the elimination so that two cells
+// share an SM (two CTAs of 8 warps, at most 128 registers per thread, one
+// copy of A per CTA in shared memory):
+//  1. Gauss-Jordan on A alone, in shared memory, in 4-column panels: warp 0
+//     picks the panel's pivots (gj_pick_pivots) and forms T^{-1}
+//     (gj_pivot_block_inverse) while the other warps copy the pivot rows'
+//     trailing columns; then every warp updates its trailing 8x8 tiles of A
+//     with one m8n8k4 FP64 MMA each (W_i -= a_i T^{-1} W_top, a_i = T_r - e_r
+//     on pivot rows), loads first, then MMAs, then stores. The panel columns
+//     are never touched again: together with T^{-1} and the pivot rows they
+//     are the record of the elimination.
+//  2. The record is replayed on [B | r_e] held in registers as 8x8 tiles
+//     (staged through the cell's own slot of XY, which the epilogue then
+//     overwrites with [X | y]): per panel the pivot rows are published and
+//     one MMA per tile applies the same update. No search runs in this phase.
+// The arithmetic is the register kernel's (the same pivots up to ties
+// within 2^-13, the same panel updates), so the results agree with the
+// reference's LU solve (src/condensation.cpp:131-148) to rounding.
+template <int Q>
+struct Gj2Cfg {
+  static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
+  static constexpr int MT = (M + 7) / 8;  // 8x8 tiles per side of A
+  // stride of A: LDA % 8 in {2, 6} makes a warp's tile loads conflict-free
+  static constexpr int LDA = ((M + 2) % 8 == 6 || (M + 2) % 8 == 2) ? M + 2 : ((M + 6) / 8) * 8 + 6;
+  static constexpr int NRT = (NR + 7) / 8;
+  static constexpr int WR = 2, WC = 4, THREADS = 32 * WR * WC;
+  static constexpr int TRW = (MT + WR - 1) / WR;   // row tiles per warp
+  static constexpr int TCA = (MT + WC - 1) / WC;   // A column tiles per warp
+  static constexpr int TCW = (NRT + WC - 1) / WC;  // right-hand-side column tiles per warp
+  static constexpr int NPAN = M / 4;
+  static constexpr int KR = (M + 31) / 32;
+  static constexpr int NP = 8 * MT, NQ = 8 * TCW * WC;
+  // A, later reused for the compact outputs (M x NR)
+  static constexpr size_t DYN = sizeof(double) * (size_t)(LDA * M > M * NR ? LDA * M : M * NR);
+};
+
+template <int Q, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    condense_gj2_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                        const double *__restrict__ r, double *XY, double *Cb, double *sf_out, double *contrib,
+                        double *panels, int *err) {
+  using C = Gj2Cfg<Q>;
+  constexpr int M = C::M, NR = C::NR, LDA = C::LDA, WR = C::WR, WC = C::WC;
+  constexpr int TRW = C::TRW, TCA = C::TCA, TCW = C::TCW, NPAN = C::NPAN, KR = C::KR;
+  constexpr int NP = C::NP, NQ = C::NQ, MT = C::MT;
+  __shared__ CondenseShared<Q> sh;
+  __shared__ double topA[4][NP];      // pivot rows of A (trailing columns) for the phase-1 update
+  __shared__ double topR[2][4][NQ];   // pivot rows of [B | r_e] in phase 2 (double-buffered)
+  __shared__ double rowbuf[KR * 32][4];
+  __shared__ double fac[NPAN][16];    // T^{-1} of every panel (row-major 4x4)
+  __shared__ int pivs[NPAN][4];
+  __shared__ int invp[KR * 32];
+  __shared__ unsigned char used[KR * 32];
+  __shared__ int sing;
+  extern __shared__ __align__(16) double A[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = warp % WR, wc = warp / WR;
+  const int gq = lane >> 2, tq = lane & 3;
+  load_tables<Q>(sh.st, tab);
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    double *Rg = XY + (size_t)e * M * NR;  // [B | r_e] staging, later [X | y]
+    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, A, Rg, e, LDA, M);
+    for (int i = threadIdx.x; i < KR * 32; i += C::THREADS) {
+      used[i] = i >= M ? 1 : 0;
+      invp[i] = 0;
+    }
+    if (threadIdx.x == 0) sing = 0;
+    __syncthreads();
+    // ------------------------------------------------ phase 1: reduce A
+#pragma unroll 1
+    for (int p = 0; p < NPAN; ++p) {
+      const int j = 4 * p;
+      double *Acol = A + (size_t)j * LDA;
+      if (warp == 0 && !gj_pick_pivots<M, KR, LDA>(j, Acol, rowbuf, pivs[p], used, invp, lane) && lane == 0)
+        sing = 1;
+      __syncthreads();
+      if (warp == 0) {
+        gj_pivot_block_inverse<LDA>(Acol, pivs[p], fac[p], lane);
+      } else {
+        // the pivot rows' trailing columns (zero left of column j + 4)
+        for (int t = threadIdx.x - 32; t < 4 * NP; t += C::THREADS - 32) {
+          const int rr = t / NP, col = t % NP;
+          topA[rr][col] = (col >= j + 4 && col < M) ? A[pivs[p][rr] + (size_t)col * LDA] : 0.;
+        }
+      }
+      __syncthreads();
+      const int tstart = (j + 4) >> 3;
+      if (tstart < MT) {
+        const double *F = fac[p];
+        const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
+        double af[TRW];
+#pragma unroll
+        for (int a = 0; a < TRW; ++a) {
+          const int row = (wr + a * WR) * 8 + gq;
+          af[a] = row < M ? -Acol[tq * LDA + row] : 0.;
+        }
+#pragma unroll
+        for (int b = 0; b < TCA; ++b) {
+          const int tj = wc + b * WC;
+          if (tj >= tstart && tj < MT) {
+            const int colb = tj * 8 + gq;
+            const double bf = f0 * topA[0][colb] + f1 * topA[1][colb] + f2 * topA[2][colb] + f3 * topA[3][colb];
+            const int col = tj * 8 + 2 * tq;
+            double d[TRW][2];
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) {
+              const int row = (wr + a * WR) * 8 + gq;
+              d[a][0] = (row < M && col < M) ? A[row + (size_t)col * LDA] : 0.;
+              d[a][1] = (row < M && col + 1 < M) ? A[row + (size_t)(col + 1) * LDA] : 0.;
+            }
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) dmma_m8n8k4(d[a][0], d[a][1], af[a], bf);
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) {
+              const int row = (wr + a * WR) * 8 + gq;
+              if (row < M && col >= j + 4 && col < M) A[row + (size_t)col * LDA] = d[a][0];
+              if (row < M && col + 1 >= j + 4 && col + 1 < M) A[row + (size_t)(col + 1) * LDA] = d[a][1];
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // ----------------------------- phase 2: replay on [B | r_e] (registers)
+    double acc[TRW][TCW][2];
+#pragma unroll
+    for (int a = 0; a < TRW; ++a) {
+      const int row = (wr + a * WR) * 8 + gq;
+#pragma unroll
+      for (int b = 0; b < TCW; ++b) {
+        const int col = (wc + b * WC) * 8 + 2 * tq;
+        acc[a][b][0] = (row < M && col < NR) ? Rg[row + (size_t)col * M] : 0.;
+        acc[a][b][1] = (row < M && col + 1 < NR) ? Rg[row + (size_t)(col + 1) * M] : 0.;
+      }
+    }
+#pragma unroll 1
+    for (int p = 0; p < NPAN; ++p) {
+      const int j = 4 * p, pb = p & 1;
+      const int pr0 = pivs[p][0], pr1 = pivs[p][1], pr2 = pivs[p][2], pr3 = pivs[p][3];
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int rbase = (wr + a * WR) * 8;
+        // warp-uniform: does this tile row hold one of the pivot rows?
+        if (!((unsigned)(pr0 - rbase) < 8u || (unsigned)(pr1 - rbase) < 8u || (unsigned)(pr2 - rbase) < 8u ||
+              (unsigned)(pr3 - rbase) < 8u))
+          continue;
+        const int row = rbase + gq;
+        const int rr = row == pr0 ? 0 : row == pr1 ? 1 : row == pr2 ? 2 : row == pr3 ? 3 : -1;
+        if (rr >= 0) {
+#pragma unroll
+          for (int b = 0; b < TCW; ++b) {
+            const int col = (wc + b * WC) * 8 + 2 * tq;
+            topR[pb][rr][col] = acc[a][b][0];
+            topR[pb][rr][col + 1] = acc[a][b][1];
+          }
+        }
+      }
+      __syncthreads();
+      const double *Acol = A + (size_t)j * LDA;
+      const double *F = fac[p];
+      const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
+      double af[TRW];
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int row = (wr + a * WR) * 8 + gq;
+        af[a] = row < M ? -Acol[tq * LDA + row] : 0.;
+      }
+#pragma unroll
+      for (int b = 0; b < TCW; ++b) {
+        const int colb = (wc + b * WC) * 8 + gq;
+        const double bf = f0 * topR[pb][0][colb] + f1 * topR[pb][1][colb] + f2 * topR[pb][2][colb] +
+                          f3 * topR[pb][3][colb];
+#pragma unroll
+        for (int a = 0; a < TRW; ++a) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf);
+      }
+    }
+    __syncthreads();  // the record in A is no longer read
+    if (sing) {
+      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
+      continue;
+    }
+    // right-hand sides back to unknown order: R(invp[w], col) = W(w, col)
+    double *R = A;  // compact M x NR, stride M
+#pragma unroll
+    for (int a = 0; a < TRW; ++a) {
+      const int row = (wr + a * WR) * 8 + gq;
+      if (row < M) {
+        const int jrow = invp[row];
+#pragma unroll
+        for (int b = 0; b < TCW; ++b) {
+          const int col = (wc + b * WC) * 8 + 2 * tq;
+          if (col < NR) R[(size_t)col * M + jrow] = acc[a][b][0];
+          if (col + 1 < NR) R[(size_t)(col + 1) * M + jrow] = acc[a][b][1];
         }
       }
     }
@@ -948,6 +1155,16 @@ static void launch_condense_gj(Ctx &c, const double *u, const double *r) {
                                             c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
 }
 
+template <int Q, int MINB>
+static void launch_condense_gj2(Ctx &c, const double *u, const double *r) {
+  using C = Gj2Cfg<Q>;
+  auto kern = condense_gj2_kernel<Q, MINB>;
+  EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
+  const int grid = std::min(c.n, sm_count_hdg() * MINB);
+  kern<<<grid, C::THREADS, C::DYN, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, r,
+                                                c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
+}
+
 template <int Q>
 static void launch_condense_gjg(Ctx &c, const double *u, const double *r) {
   using C = GjgCfg<Q>;
@@ -973,7 +1190,7 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
     case 2: launch_condense_gj<2, 1, 2, 6>(c, u, r); break;
     case 3: launch_condense_gj<3, 2, 2, 4>(c, u, r); break;
     case 4: launch_condense_gj<4, 2, 4, 2>(c, u, r); break;
-    case 5: launch_condense_gj<5, 2, 4, 1>(c, u, r); break;
+    case 5: launch_condense_gj2<5, 2>(c, u, r); break;
     case 6: launch_condense_gjg<6>(c, u, r); break;
     case 7: launch_condense_gjg<7>(c, u, r); break;
     case 8: launch_condense_gjg<8>(c, u, r); break;

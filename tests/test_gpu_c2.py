@@ -5,8 +5,11 @@ update, for HDG with block Jacobi and block ILU(0) and for DG with block
 Jacobi.
 
 Per update (every _iterations.csv row): step/stage/newton indices and the
-line-search damping identical, the physical residual rms within 1e-8
-relative, dt within 1e-12, Krylov counts within two iterations. Final state:
+line-search damping identical; the physical residual rms within 1e-8 of the
+stage's first rms, and within 1e-8 of itself where it is above 1e-6 of that
+(the third update of a stage reaches ~1e-13, the roundoff floor of the
+residual, where either code's rms is rounding noise); dt within 1e-12;
+Krylov counts within two iterations. Final state:
 every 32nd coefficient within 1e-10 relative and the per-component sums of
 squares within 1e-10; L2 errors within 1e-9 relative; conservation drift
 within 1e-13 of the reference's own (1.12e-12 here: with three Newton updates
@@ -46,7 +49,12 @@ def test_headline_workload_update_by_update(path, tmp_path):
         np.testing.assert_array_equal(iters[:, c[name]], ref[:, c[name]])
     np.testing.assert_array_equal(iters[:, c["damping"]], ref[:, c["damping"]])
     rms, ref_rms = iters[:, c["residual_physical_rms"]], ref[:, c["residual_physical_rms"]]
-    assert np.max(np.abs(rms - ref_rms) / np.abs(ref_rms)) < 1e-8
+    # scale of each row: the rms at the stage's first update
+    first = np.where(ref[:, c["newton"]] == 0)[0]
+    scale = ref_rms[first[np.searchsorted(first, np.arange(len(ref_rms)), side="right") - 1]]
+    assert np.max(np.abs(rms - ref_rms) / scale) < 1e-8
+    above = ref_rms >= 1e-6 * scale
+    assert np.max(np.abs(rms - ref_rms)[above] / ref_rms[above]) < 1e-8
     assert np.max(np.abs(iters[:, c["dt"]] - ref[:, c["dt"]]) / ref[:, c["dt"]]) < 1e-12
     assert np.all(np.abs(iters[:, c["krylov_iterations"]] - ref[:, c["krylov_iterations"]]) <= 2)
     coeff = np.loadtxt(f"{prefix}_{form}_coefficients.csv", delimiter=",", skiprows=1)
