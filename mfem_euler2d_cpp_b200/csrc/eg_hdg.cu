@@ -100,6 +100,7 @@ __device__ void condense_build(CondenseShared<Q> &sh, const Geo &g, const Frozen
   }
   __syncthreads();
   build_cell_matrix<Q>(A, ld, st, sh.us, sh.FM, g);
+  if (R == nullptr) return;  // the caller forms [B | r_e] itself (lift_entry)
   for (int col = threadIdx.x; col < NR; col += blockDim.x) {
     double *rc = R + (size_t)col * ldr;
     if (col < 4 * T) {
@@ -165,6 +166,71 @@ __device__ void condense_epilogue(const CondenseShared<Q> &sh, const double *R, 
 #pragma unroll
       for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * val[d];
       panels[(size_t)e * npan * T * T + o] = res;
+    }
+  }
+}
+
+// Entry (row, col) of the lift B (col < 4t) of the cell system: the face
+// point's scalar lift sf times phi * inv_mass on the component of the column
+// (HybridCell's B, src/problem.cpp:622-630; the same values condense_build
+// writes). SF is the cell's staged lift scalars.
+template <int Q>
+__device__ __forceinline__ double lift_entry(const STab<Q> &st, const double *SF, int row, int col) {
+  constexpr int T = 4 * Q;
+  const int s = col / T, rem = col % T, jj = rem >> 2, c = rem & 3;
+  const int i = row >> 2;
+  if ((row & 3) != c) return 0.;
+  const int ix = i % Q, iy = i / Q;
+  const bool on = s < 2 ? iy == jj : ix == jj;
+  if (!on) return 0.;
+  const int l = s < 2 ? ix : iy;
+  return st.fb(s, jj, l) * st.inv_mass(i) * SF[s * Q + jj];
+}
+
+// Outputs of a solved cell from R = [X | y] (stride ldr, unknown order):
+// [X | y] to XY (compact), the trace contributions C_e y_e and the Schur
+// panels C_s X_o (src/condensation.cpp:141-142, src/operators.cpp:7-26). One
+// thread per (side, column) forms the column's trace on the side once
+// (q face points x 4 components) and applies the side's 4x4 flux blocks,
+// emitting 4q consecutive outputs.
+template <int Q>
+__device__ void condense_epilogue_traces(const CondenseShared<Q> &sh, const double *R, int ldr, double *XY,
+                                         double *contrib, double *panels, int npan, int e) {
+  constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
+  const STab<Q> &st = sh.st;
+  double *dst = XY + (size_t)e * M * NR;
+  for (int i = threadIdx.x; i < M * NR; i += blockDim.x) dst[i] = R[(size_t)(i / M) * ldr + i % M];
+  const bool all16 = npan == 16;
+  for (int task = threadIdx.x; task < 4 * NR; task += blockDim.x) {
+    const int s = task & 3, col = task >> 2;
+    const int so = col / T;  // block column of X (4 = y)
+    if (col < 4 * T && !all16 && so != s) continue;
+    double *out;
+    if (col == 4 * T) {
+      out = contrib + (size_t)e * 4 * T + s * T;
+    } else {
+      if (panels == nullptr) continue;
+      const int pan = all16 ? s * 4 + so : s;
+      out = panels + (((size_t)e * npan + pan) * T + (col - so * T)) * T;
+    }
+    const double *xc = R + (size_t)col * ldr;
+    for (int jj = 0; jj < Q; ++jj) {
+      double v[4] = {0., 0., 0., 0.};
+#pragma unroll
+      for (int l = 0; l < Q; ++l) {
+        const double f = st.fb(s, jj, l);
+        const double *xv = xc + 4 * line_node<Q>(s, jj, l);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) v[d] += f * xv[d];
+      }
+      const double *cb = sh.CB + (s * Q + jj) * 16;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        double res = 0.;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) res += cb[c + 4 * d] * v[d];
+        out[jj * 4 + c] = res;
+      }
     }
   }
 }
@@ -402,8 +468,9 @@ struct Gj2Cfg {
   static constexpr int NPAN = M / 4;
   static constexpr int KR = (M + 31) / 32;
   static constexpr int NP = 8 * MT, NQ = 8 * TCW * WC;
-  // A, later reused for the compact outputs (M x NR)
-  static constexpr size_t DYN = sizeof(double) * (size_t)(LDA * M > M * NR ? LDA * M : M * NR);
+  // A, later reused for the outputs (M x NR at stride M + 1)
+  static constexpr size_t DYN =
+      sizeof(double) * (size_t)(LDA * M > (M + 1) * NR ? LDA * M : (M + 1) * NR);
 };
 
 template <int Q, int MINB>
@@ -431,8 +498,15 @@ __global__ void __launch_bounds__(256, MINB)
   load_tables<Q>(sh.st, tab);
   for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
     __syncthreads();
-    double *Rg = XY + (size_t)e * M * NR;  // [B | r_e] staging, later [X | y]
-    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, A, Rg, e, LDA, M);
+    condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, A, nullptr, e, LDA);
+    // [B | r_e] staged in the cell's slot of XY (L2-resident until [X | y]
+    // overwrites it), one element per thread in address order
+    double *Rg = XY + (size_t)e * M * NR;
+    const double *re = r + (size_t)e * M;
+    for (int i = threadIdx.x; i < M * NR; i += C::THREADS) {
+      const int col = i / M, row = i % M;
+      Rg[i] = col == NR - 1 ? re[row] : lift_entry<Q>(sh.st, sh.SF, row, col);
+    }
     for (int i = threadIdx.x; i < KR * 32; i += C::THREADS) {
       used[i] = i >= M ? 1 : 0;
       invp[i] = 0;
@@ -553,7 +627,7 @@ __global__ void __launch_bounds__(256, MINB)
       continue;
     }
     // right-hand sides back to unknown order: R(invp[w], col) = W(w, col)
-    double *R = A;  // compact M x NR, stride M
+    double *R = A;  // M x NR, odd stride M + 1 (conflict-free column reads in the epilogue)
 #pragma unroll
     for (int a = 0; a < TRW; ++a) {
       const int row = (wr + a * WR) * 8 + gq;
@@ -562,13 +636,13 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
         for (int b = 0; b < TCW; ++b) {
           const int col = (wc + b * WC) * 8 + 2 * tq;
-          if (col < NR) R[(size_t)col * M + jrow] = acc[a][b][0];
-          if (col + 1 < NR) R[(size_t)(col + 1) * M + jrow] = acc[a][b][1];
+          if (col < NR) R[(size_t)col * (M + 1) + jrow] = acc[a][b][0];
+          if (col + 1 < NR) R[(size_t)(col + 1) * (M + 1) + jrow] = acc[a][b][1];
         }
       }
     }
     __syncthreads();
-    condense_epilogue<Q>(sh, R, true, XY, contrib, panels, g.npan, e);
+    condense_epilogue_traces<Q>(sh, R, M + 1, XY, contrib, panels, g.npan, e);
   }
 }
 
@@ -1189,7 +1263,7 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
     case 1: launch_condense_gj<1, 1, 1, 8>(c, u, r); break;
     case 2: launch_condense_gj<2, 1, 2, 6>(c, u, r); break;
     case 3: launch_condense_gj<3, 2, 2, 4>(c, u, r); break;
-    case 4: launch_condense_gj<4, 2, 4, 2>(c, u, r); break;
+    case 4: launch_condense_gj2<4, 3>(c, u, r); break;
     case 5: launch_condense_gj2<5, 2>(c, u, r); break;
     case 6: launch_condense_gjg<6>(c, u, r); break;
     case 7: launch_condense_gjg<7>(c, u, r); break;
