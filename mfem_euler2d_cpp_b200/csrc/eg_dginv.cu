@@ -194,6 +194,89 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
   }
 }
 
+// The two-phase form of the same inverse (eg_gj.cuh gj2_reduce/gj2_replay):
+// phase 1 reduces the block in shared memory with two CTAs per SM, phase 2
+// replays the recorded panels on the identity, 64 columns per pass. The
+// result W has its rows in pivot order -- row w holds row perm[w] of the
+// inverse -- and is stored column-major as it leaves the registers; the
+// apply scatters through perm.
+template <int Q, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    dg_inverse_gj2_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                          double *__restrict__ inv, int *__restrict__ perm, int *err) {
+  constexpr int M = 4 * Q * Q;
+  using C = Gj2Cfg<M, M>;
+  constexpr int WR = C::WR, WC = C::WC, TRW = C::TRW, NPAN = C::NPAN, KR = C::KR, NP = C::NP, LDA = C::LDA;
+  constexpr int TCB = 2, CBW = 8 * TCB * WC, NPASS = (M + CBW - 1) / CBW;
+  __shared__ STab<Q> st;
+  __shared__ double us[M], UT[16 * Q], FM[4 * Q * 16];
+  __shared__ double topA[4][NP];
+  __shared__ double topR[2][4][CBW];
+  __shared__ double rowbuf[KR * 32][4];
+  __shared__ double fac[NPAN][16];
+  __shared__ int pivs[NPAN][4];
+  __shared__ int invp[KR * 32];
+  __shared__ unsigned char used[KR * 32];
+  __shared__ int sing;
+  extern __shared__ __align__(16) double A[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = warp % WR, wc = warp / WR;
+  const int gq = lane >> 2, tq = lane & 3;
+  load_tables<Q>(st, tab);
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < M; i += C::THREADS) us[i] = u[(size_t)e * M + i];
+    __syncthreads();
+    cell_traces<Q>(st, us, UT);
+    __syncthreads();
+    dg_face_matrices<Q>(UT, FM, g, fz, e);
+    __syncthreads();
+    build_cell_matrix<Q>(A, LDA, st, us, FM, g);
+    for (int i = threadIdx.x; i < KR * 32; i += C::THREADS) {
+      used[i] = i >= M ? 1 : 0;
+      invp[i] = 0;
+    }
+    if (threadIdx.x == 0) sing = 0;
+    __syncthreads();
+    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing);
+    double *W = inv + (size_t)e * M * M;
+#pragma unroll 1
+    for (int pass = 0; pass < NPASS; ++pass) {
+      const int c0 = pass * CBW;
+      double acc[TRW][TCB][2];
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int row = (wr + a * WR) * 8 + gq;
+#pragma unroll
+        for (int b = 0; b < TCB; ++b) {
+          const int col = c0 + (wc + b * WC) * 8 + 2 * tq;
+          acc[a][b][0] = (row < M && col == row) ? 1. : 0.;
+          acc[a][b][1] = (row < M && col + 1 == row) ? 1. : 0.;
+        }
+      }
+      gj2_replay<C, TCB>(A, fac, pivs, topR, acc);
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int row = (wr + a * WR) * 8 + gq;
+        if (row < M) {
+#pragma unroll
+          for (int b = 0; b < TCB; ++b) {
+            const int col = c0 + (wc + b * WC) * 8 + 2 * tq;
+            if (col < M) W[(size_t)col * M + row] = acc[a][b][0];
+            if (col + 1 < M) W[(size_t)(col + 1) * M + row] = acc[a][b][1];
+          }
+        }
+      }
+      __syncthreads();  // topR is reused by the next pass
+    }
+    if (sing) {
+      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_JACOBI);
+      continue;
+    }
+    for (int i = threadIdx.x; i < M; i += C::THREADS) perm[(size_t)e * M + i] = invp[i];
+  }
+}
+
 // x_e = A_e^{-1} b_e, inverses column-major: one warp per cell, lane l holds
 // rows 2l, 2l+1 (+ 64 s); the right-hand side is staged per warp in shared
 // memory and broadcast column by column.
@@ -201,7 +284,8 @@ template <int M>
 __global__ void __launch_bounds__(256) block_inverse_cm_apply_kernel(const double *__restrict__ inv, int nblocks,
                                                                      const double *__restrict__ b,
                                                                      double *__restrict__ x,
-                                                                     const int *__restrict__ skip) {
+                                                                     const int *__restrict__ skip,
+                                                                     const int *__restrict__ perm) {
   if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
   constexpr int S = (M + 63) / 64;
   __shared__ double bs[8][M];
@@ -231,7 +315,15 @@ __global__ void __launch_bounds__(256) block_inverse_cm_apply_kernel(const doubl
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int r2 = lane + 32 * s;
-    if (2 * r2 < M) reinterpret_cast<double2 *>(x + (size_t)blk * M)[r2] = make_double2(acc[s][0], acc[s][1]);
+    if (2 * r2 < M) {
+      if (perm == nullptr) {
+        reinterpret_cast<double2 *>(x + (size_t)blk * M)[r2] = make_double2(acc[s][0], acc[s][1]);
+      } else {  // row w of the stored inverse is row perm[w] of the true one
+        const int *pb = perm + (size_t)blk * M;
+        x[(size_t)blk * M + pb[2 * r2]] = acc[s][0];
+        x[(size_t)blk * M + pb[2 * r2 + 1]] = acc[s][1];
+      }
+    }
   }
 }
 
@@ -258,9 +350,21 @@ void launch_inverse(Ctx &c, const double *u) {
   EG_CUDA(cudaGetLastError());
 }
 
+template <int Q, int MINB>
+void launch_inverse2(Ctx &c, const double *u) {
+  using C = Gj2Cfg<4 * Q * Q, 4 * Q * Q>;
+  auto kern = dg_inverse_gj2_kernel<Q, MINB>;
+  EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
+  const int grid = std::min(c.n, sm_count_dginv() * MINB);
+  kern<<<grid, C::THREADS, C::DYN, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, c.pc_dg,
+                                                c.piv_dg, c.derr);
+  EG_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 
 bool dg_inverse_supported(int q) { return q >= 1 && q <= 5; }
+bool dg_inverse_permuted(int q) { return q >= 4; }
 
 void launch_dg_inverse(Ctx &c, const double *u) {
   c.ensure_pc_dg();
@@ -269,8 +373,8 @@ void launch_dg_inverse(Ctx &c, const double *u) {
     case 1: launch_inverse<1, 1, 1, 8>(c, u); break;
     case 2: launch_inverse<2, 1, 2, 4>(c, u); break;
     case 3: launch_inverse<3, 2, 2, 2>(c, u); break;
-    case 4: launch_inverse<4, 2, 4, 1>(c, u); break;
-    case 5: launch_inverse<5, 2, 4, 1>(c, u); break;
+    case 4: launch_inverse2<4, 3>(c, u); break;
+    case 5: launch_inverse2<5, 2>(c, u); break;
     default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 4");
   }
 }
@@ -278,12 +382,13 @@ void launch_dg_inverse(Ctx &c, const double *u) {
 void launch_dg_inverse_apply(Ctx &c, const double *b, double *x) {
   ProfScope ps(c, EG_K_PC_APPLY, 1);
   const int grid = (c.n + 7) / 8;
+  const int *perm = dg_inverse_permuted(c.q) ? c.piv_dg : nullptr;
   switch (c.q) {
-    case 1: block_inverse_cm_apply_kernel<4><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip); break;
-    case 2: block_inverse_cm_apply_kernel<16><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip); break;
-    case 3: block_inverse_cm_apply_kernel<36><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip); break;
-    case 4: block_inverse_cm_apply_kernel<64><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip); break;
-    case 5: block_inverse_cm_apply_kernel<100><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip); break;
+    case 1: block_inverse_cm_apply_kernel<4><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
+    case 2: block_inverse_cm_apply_kernel<16><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
+    case 3: block_inverse_cm_apply_kernel<36><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
+    case 4: block_inverse_cm_apply_kernel<64><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
+    case 5: block_inverse_cm_apply_kernel<100><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
     default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 4");
   }
   EG_CUDA(cudaGetLastError());

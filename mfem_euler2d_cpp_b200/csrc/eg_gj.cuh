@@ -287,4 +287,152 @@ __device__ __forceinline__ void gj_pivot_block_inverse(double *Acol, const int *
   if (lane < 4) Acol[lane * LDA + pivs[lane]] -= 1.;
 }
 
+// Shapes of the two-phase Gauss-Jordan for an M x M cell matrix and NR
+// right-hand sides (8 warps: 2 x 4 over 8x8 tiles).
+template <int M_, int NR_>
+struct Gj2Cfg {
+  static constexpr int M = M_, NR = NR_;
+  static constexpr int MT = (M + 7) / 8;  // 8x8 tiles per side of A
+  // stride of A: LDA % 8 in {2, 6} makes a warp's tile loads conflict-free
+  static constexpr int LDA = ((M + 2) % 8 == 6 || (M + 2) % 8 == 2) ? M + 2 : ((M + 6) / 8) * 8 + 6;
+  static constexpr int NRT = (NR + 7) / 8;
+  static constexpr int WR = 2, WC = 4, THREADS = 32 * WR * WC;
+  static constexpr int TRW = (MT + WR - 1) / WR;   // row tiles per warp
+  static constexpr int TCA = (MT + WC - 1) / WC;   // A column tiles per warp
+  static constexpr int TCW = (NRT + WC - 1) / WC;  // right-hand-side column tiles per warp
+  static constexpr int NPAN = M / 4;
+  static constexpr int KR = (M + 31) / 32;
+  static constexpr int NP = 8 * MT, NQ = 8 * TCW * WC;
+  // A, later reused for the outputs (M x NR at stride M + 1)
+  static constexpr size_t DYN =
+      sizeof(double) * (size_t)(LDA * M > (M + 1) * NR ? LDA * M : (M + 1) * NR);
+};
+
+// Phase 1 of the two-phase Gauss-Jordan (C: a Gj2Cfg): reduce the cell
+// matrix A (shared memory, column-major, stride C::LDA) in 4-column panels
+// with row partial pivoting. Warp 0 picks each panel's pivots and forms
+// T^{-1}; the other warps copy the pivot rows' trailing columns; then every
+// warp updates its trailing 8x8 tiles with one m8n8k4 FP64 MMA each
+// (W_i -= a_i T^{-1} W_top, a_i = T_r - e_r on pivot rows), loads first,
+// then MMAs, then stores. The panel columns are never written again:
+// together with fac (T^{-1}) and pivs they record the elimination.
+template <class C>
+__device__ __forceinline__ void gj2_reduce(double *A, double (*topA)[C::NP], double (*rowbuf)[4], double (*fac)[16],
+                                           int (*pivs)[4], unsigned char *used, int *invp, int *sing) {
+  constexpr int M = C::M, LDA = C::LDA, WR = C::WR, WC = C::WC, TRW = C::TRW, TCA = C::TCA;
+  constexpr int NPAN = C::NPAN, KR = C::KR, NP = C::NP, MT = C::MT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = warp % WR, wc = warp / WR;
+  const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll 1
+    for (int p = 0; p < NPAN; ++p) {
+      const int j = 4 * p;
+      double *Acol = A + (size_t)j * LDA;
+      if (warp == 0 && !gj_pick_pivots<M, KR, LDA>(j, Acol, rowbuf, pivs[p], used, invp, lane) && lane == 0)
+        *sing = 1;
+      __syncthreads();
+      if (warp == 0) {
+        gj_pivot_block_inverse<LDA>(Acol, pivs[p], fac[p], lane);
+      } else {
+        // the pivot rows' trailing columns (zero left of column j + 4)
+        for (int t = threadIdx.x - 32; t < 4 * NP; t += C::THREADS - 32) {
+          const int rr = t / NP, col = t % NP;
+          topA[rr][col] = (col >= j + 4 && col < M) ? A[pivs[p][rr] + (size_t)col * LDA] : 0.;
+        }
+      }
+      __syncthreads();
+      const int tstart = (j + 4) >> 3;
+      if (tstart < MT) {
+        const double *F = fac[p];
+        const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
+        double af[TRW];
+#pragma unroll
+        for (int a = 0; a < TRW; ++a) {
+          const int row = (wr + a * WR) * 8 + gq;
+          af[a] = row < M ? -Acol[tq * LDA + row] : 0.;
+        }
+#pragma unroll
+        for (int b = 0; b < TCA; ++b) {
+          const int tj = wc + b * WC;
+          if (tj >= tstart && tj < MT) {
+            const int colb = tj * 8 + gq;
+            const double bf = f0 * topA[0][colb] + f1 * topA[1][colb] + f2 * topA[2][colb] + f3 * topA[3][colb];
+            const int col = tj * 8 + 2 * tq;
+            double d[TRW][2];
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) {
+              const int row = (wr + a * WR) * 8 + gq;
+              d[a][0] = (row < M && col < M) ? A[row + (size_t)col * LDA] : 0.;
+              d[a][1] = (row < M && col + 1 < M) ? A[row + (size_t)(col + 1) * LDA] : 0.;
+            }
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) dmma_m8n8k4(d[a][0], d[a][1], af[a], bf);
+#pragma unroll
+            for (int a = 0; a < TRW; ++a) {
+              const int row = (wr + a * WR) * 8 + gq;
+              if (row < M && col >= j + 4 && col < M) A[row + (size_t)col * LDA] = d[a][0];
+              if (row < M && col + 1 >= j + 4 && col + 1 < M) A[row + (size_t)(col + 1) * LDA] = d[a][1];
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+// Phase 2: replay the recorded panels on right-hand sides held in registers
+// as the warp's 8x8 tiles (rows (wr + a WR) 8 + gq, columns (wc + b WC) 8 +
+// 2 tq + h): per panel the pivot rows are published (topR, double-buffered)
+// and one MMA per tile applies the panel's update. Leaves the rows in pivot
+// order: row w holds unknown invp[w].
+template <class C, int TCW>
+__device__ __forceinline__ void gj2_replay(const double *A, const double (*fac)[16], const int (*pivs)[4],
+                                           double (*topR)[4][8 * TCW * C::WC], double (&acc)[C::TRW][TCW][2]) {
+  constexpr int M = C::M, LDA = C::LDA, WR = C::WR, WC = C::WC, TRW = C::TRW, NPAN = C::NPAN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = warp % WR, wc = warp / WR;
+  const int gq = lane >> 2, tq = lane & 3;
+#pragma unroll 1
+    for (int p = 0; p < NPAN; ++p) {
+      const int j = 4 * p, pb = p & 1;
+      const int pr0 = pivs[p][0], pr1 = pivs[p][1], pr2 = pivs[p][2], pr3 = pivs[p][3];
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int rbase = (wr + a * WR) * 8;
+        // warp-uniform: does this tile row hold one of the pivot rows?
+        if (!((unsigned)(pr0 - rbase) < 8u || (unsigned)(pr1 - rbase) < 8u || (unsigned)(pr2 - rbase) < 8u ||
+              (unsigned)(pr3 - rbase) < 8u))
+          continue;
+        const int row = rbase + gq;
+        const int rr = row == pr0 ? 0 : row == pr1 ? 1 : row == pr2 ? 2 : row == pr3 ? 3 : -1;
+        if (rr >= 0) {
+#pragma unroll
+          for (int b = 0; b < TCW; ++b) {
+            const int col = (wc + b * WC) * 8 + 2 * tq;
+            topR[pb][rr][col] = acc[a][b][0];
+            topR[pb][rr][col + 1] = acc[a][b][1];
+          }
+        }
+      }
+      __syncthreads();
+      const double *Acol = A + (size_t)j * LDA;
+      const double *F = fac[p];
+      const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
+      double af[TRW];
+#pragma unroll
+      for (int a = 0; a < TRW; ++a) {
+        const int row = (wr + a * WR) * 8 + gq;
+        af[a] = row < M ? -Acol[tq * LDA + row] : 0.;
+      }
+#pragma unroll
+      for (int b = 0; b < TCW; ++b) {
+        const int colb = (wc + b * WC) * 8 + gq;
+        const double bf = f0 * topR[pb][0][colb] + f1 * topR[pb][1][colb] + f2 * topR[pb][2][colb] +
+                          f3 * topR[pb][3][colb];
+#pragma unroll
+        for (int a = 0; a < TRW; ++a) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf);
+      }
+    }
+}
+
 }  // namespace eg

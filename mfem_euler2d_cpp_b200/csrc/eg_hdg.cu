@@ -454,34 +454,15 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
 // The arithmetic is the register kernel's (the same pivots up to ties
 // within 2^-13, the same panel updates), so the results agree with the
 // reference's LU solve (src/condensation.cpp:131-148) to rounding.
-template <int Q>
-struct Gj2Cfg {
-  static constexpr int P = Q * Q, M = 4 * P, T = 4 * Q, NR = 4 * T + 1;
-  static constexpr int MT = (M + 7) / 8;  // 8x8 tiles per side of A
-  // stride of A: LDA % 8 in {2, 6} makes a warp's tile loads conflict-free
-  static constexpr int LDA = ((M + 2) % 8 == 6 || (M + 2) % 8 == 2) ? M + 2 : ((M + 6) / 8) * 8 + 6;
-  static constexpr int NRT = (NR + 7) / 8;
-  static constexpr int WR = 2, WC = 4, THREADS = 32 * WR * WC;
-  static constexpr int TRW = (MT + WR - 1) / WR;   // row tiles per warp
-  static constexpr int TCA = (MT + WC - 1) / WC;   // A column tiles per warp
-  static constexpr int TCW = (NRT + WC - 1) / WC;  // right-hand-side column tiles per warp
-  static constexpr int NPAN = M / 4;
-  static constexpr int KR = (M + 31) / 32;
-  static constexpr int NP = 8 * MT, NQ = 8 * TCW * WC;
-  // A, later reused for the outputs (M x NR at stride M + 1)
-  static constexpr size_t DYN =
-      sizeof(double) * (size_t)(LDA * M > (M + 1) * NR ? LDA * M : (M + 1) * NR);
-};
-
 template <int Q, int MINB>
 __global__ void __launch_bounds__(256, MINB)
     condense_gj2_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
                         const double *__restrict__ r, double *XY, double *Cb, double *sf_out, double *contrib,
                         double *panels, int *err) {
-  using C = Gj2Cfg<Q>;
-  constexpr int M = C::M, NR = C::NR, LDA = C::LDA, WR = C::WR, WC = C::WC;
-  constexpr int TRW = C::TRW, TCA = C::TCA, TCW = C::TCW, NPAN = C::NPAN, KR = C::KR;
-  constexpr int NP = C::NP, NQ = C::NQ, MT = C::MT;
+  using C = Gj2Cfg<4 * Q * Q, 16 * Q + 1>;
+  constexpr int M = C::M, NR = C::NR, WR = C::WR, WC = C::WC;
+  constexpr int TRW = C::TRW, TCW = C::TCW, NPAN = C::NPAN, KR = C::KR;
+  constexpr int NP = C::NP, NQ = C::NQ, LDA = C::LDA;
   __shared__ CondenseShared<Q> sh;
   __shared__ double topA[4][NP];      // pivot rows of A (trailing columns) for the phase-1 update
   __shared__ double topR[2][4][NQ];   // pivot rows of [B | r_e] in phase 2 (double-buffered)
@@ -514,60 +495,7 @@ __global__ void __launch_bounds__(256, MINB)
     if (threadIdx.x == 0) sing = 0;
     __syncthreads();
     // ------------------------------------------------ phase 1: reduce A
-#pragma unroll 1
-    for (int p = 0; p < NPAN; ++p) {
-      const int j = 4 * p;
-      double *Acol = A + (size_t)j * LDA;
-      if (warp == 0 && !gj_pick_pivots<M, KR, LDA>(j, Acol, rowbuf, pivs[p], used, invp, lane) && lane == 0)
-        sing = 1;
-      __syncthreads();
-      if (warp == 0) {
-        gj_pivot_block_inverse<LDA>(Acol, pivs[p], fac[p], lane);
-      } else {
-        // the pivot rows' trailing columns (zero left of column j + 4)
-        for (int t = threadIdx.x - 32; t < 4 * NP; t += C::THREADS - 32) {
-          const int rr = t / NP, col = t % NP;
-          topA[rr][col] = (col >= j + 4 && col < M) ? A[pivs[p][rr] + (size_t)col * LDA] : 0.;
-        }
-      }
-      __syncthreads();
-      const int tstart = (j + 4) >> 3;
-      if (tstart < MT) {
-        const double *F = fac[p];
-        const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
-        double af[TRW];
-#pragma unroll
-        for (int a = 0; a < TRW; ++a) {
-          const int row = (wr + a * WR) * 8 + gq;
-          af[a] = row < M ? -Acol[tq * LDA + row] : 0.;
-        }
-#pragma unroll
-        for (int b = 0; b < TCA; ++b) {
-          const int tj = wc + b * WC;
-          if (tj >= tstart && tj < MT) {
-            const int colb = tj * 8 + gq;
-            const double bf = f0 * topA[0][colb] + f1 * topA[1][colb] + f2 * topA[2][colb] + f3 * topA[3][colb];
-            const int col = tj * 8 + 2 * tq;
-            double d[TRW][2];
-#pragma unroll
-            for (int a = 0; a < TRW; ++a) {
-              const int row = (wr + a * WR) * 8 + gq;
-              d[a][0] = (row < M && col < M) ? A[row + (size_t)col * LDA] : 0.;
-              d[a][1] = (row < M && col + 1 < M) ? A[row + (size_t)(col + 1) * LDA] : 0.;
-            }
-#pragma unroll
-            for (int a = 0; a < TRW; ++a) dmma_m8n8k4(d[a][0], d[a][1], af[a], bf);
-#pragma unroll
-            for (int a = 0; a < TRW; ++a) {
-              const int row = (wr + a * WR) * 8 + gq;
-              if (row < M && col >= j + 4 && col < M) A[row + (size_t)col * LDA] = d[a][0];
-              if (row < M && col + 1 >= j + 4 && col + 1 < M) A[row + (size_t)(col + 1) * LDA] = d[a][1];
-            }
-          }
-        }
-      }
-      __syncthreads();
-    }
+    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing);
     // ----------------------------- phase 2: replay on [B | r_e] (registers)
     double acc[TRW][TCW][2];
 #pragma unroll
@@ -580,47 +508,7 @@ __global__ void __launch_bounds__(256, MINB)
         acc[a][b][1] = (row < M && col + 1 < NR) ? Rg[row + (size_t)(col + 1) * M] : 0.;
       }
     }
-#pragma unroll 1
-    for (int p = 0; p < NPAN; ++p) {
-      const int j = 4 * p, pb = p & 1;
-      const int pr0 = pivs[p][0], pr1 = pivs[p][1], pr2 = pivs[p][2], pr3 = pivs[p][3];
-#pragma unroll
-      for (int a = 0; a < TRW; ++a) {
-        const int rbase = (wr + a * WR) * 8;
-        // warp-uniform: does this tile row hold one of the pivot rows?
-        if (!((unsigned)(pr0 - rbase) < 8u || (unsigned)(pr1 - rbase) < 8u || (unsigned)(pr2 - rbase) < 8u ||
-              (unsigned)(pr3 - rbase) < 8u))
-          continue;
-        const int row = rbase + gq;
-        const int rr = row == pr0 ? 0 : row == pr1 ? 1 : row == pr2 ? 2 : row == pr3 ? 3 : -1;
-        if (rr >= 0) {
-#pragma unroll
-          for (int b = 0; b < TCW; ++b) {
-            const int col = (wc + b * WC) * 8 + 2 * tq;
-            topR[pb][rr][col] = acc[a][b][0];
-            topR[pb][rr][col + 1] = acc[a][b][1];
-          }
-        }
-      }
-      __syncthreads();
-      const double *Acol = A + (size_t)j * LDA;
-      const double *F = fac[p];
-      const double f0 = F[4 * tq], f1 = F[4 * tq + 1], f2 = F[4 * tq + 2], f3 = F[4 * tq + 3];
-      double af[TRW];
-#pragma unroll
-      for (int a = 0; a < TRW; ++a) {
-        const int row = (wr + a * WR) * 8 + gq;
-        af[a] = row < M ? -Acol[tq * LDA + row] : 0.;
-      }
-#pragma unroll
-      for (int b = 0; b < TCW; ++b) {
-        const int colb = (wc + b * WC) * 8 + gq;
-        const double bf = f0 * topR[pb][0][colb] + f1 * topR[pb][1][colb] + f2 * topR[pb][2][colb] +
-                          f3 * topR[pb][3][colb];
-#pragma unroll
-        for (int a = 0; a < TRW; ++a) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf);
-      }
-    }
+    gj2_replay<C, TCW>(A, fac, pivs, topR, acc);
     __syncthreads();  // the record in A is no longer read
     if (sing) {
       if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_CELL);
@@ -1231,7 +1119,7 @@ static void launch_condense_gj(Ctx &c, const double *u, const double *r) {
 
 template <int Q, int MINB>
 static void launch_condense_gj2(Ctx &c, const double *u, const double *r) {
-  using C = Gj2Cfg<Q>;
+  using C = Gj2Cfg<4 * Q * Q, 16 * Q + 1>;
   auto kern = condense_gj2_kernel<Q, MINB>;
   EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
   const int grid = std::min(c.n, sm_count_hdg() * MINB);

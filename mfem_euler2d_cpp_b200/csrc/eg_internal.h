@@ -264,6 +264,9 @@ void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblock
 void launch_dg_jacobi_apply(Ctx &c, const double *b, double *x);
 // ---- explicit DG block-Jacobi inverses (eg_dginv.cu) ----
 bool dg_inverse_supported(int q);
+// with q >= 4 the stored inverse has its rows in pivot order: row w is row
+// piv_dg[e*m + w] of the cell's true inverse
+bool dg_inverse_permuted(int q);
 void launch_dg_inverse(Ctx &c, const double *u);  // pc_dg <- column-major J_KK^{-1}
 void launch_dg_inverse_apply(Ctx &c, const double *b, double *x);
 // ---- launchers (eg_hdg.cu) ----

@@ -258,3 +258,28 @@ def test_high_degree_condensation_on_many_cells(condense_case, precision):
         v, lam = vrng.standard_normal(ctx.nl), vrng.standard_normal(ctx.nl)
         assert rel_err(ctx.schur_apply(v), f["sv"]) < OP_TOL
         assert rel_err(ctx.recover(lam), f["du"]) < OP_TOL
+
+
+@pytest.mark.parametrize("nx,ny,k", [(12, 10, 1), (10, 8, 2), (6, 5, 3), (5, 6, 4)])
+def test_dg_pc_blocks_are_inverses(nx, ny, k):
+    """After eg_pc_factor(1) the DG block-Jacobi slot holds each cell block's
+    explicit inverse, column-major (the k >= 3 factor keeps its rows in pivot
+    order on the device; the download restores them): inverse x block = I."""
+    d = capi.simple_wave_desc(nx, ny, k, 37.0)
+    with capi.Context(d, capi.default_opts(form=capi.FORM_DG)) as ctx:
+        ctx.initial()
+        rate = ctx.freeze(1e-3)
+        ctx.freeze(0.24 / rate)
+        ctx.upload("OLD", ctx.download("U") * 0.999)
+        ctx.set_dt(0.24 / rate)
+        m = ctx.nu // (nx * ny)
+        ctx.pc_factor(False)
+        blocks = ctx.download("PC_BLOCKS").reshape(nx * ny, m, m).transpose(0, 2, 1)
+        ctx.pc_factor(True)
+        inv = ctx.download("PC_BLOCKS").reshape(nx * ny, m, m).transpose(0, 2, 1)
+        prod = np.einsum("eij,ejk->eik", inv, blocks)
+        err = np.abs(prod - np.eye(m)).max(axis=(1, 2)) / (np.abs(inv).max(axis=(1, 2)) * np.abs(blocks).max(axis=(1, 2)))
+        assert err.max() < 1e-13
+        b = np.cos(0.3 * np.arange(ctx.nu))
+        want = np.einsum("eij,ej->ei", inv, b.reshape(nx * ny, m)).ravel()
+        assert rel_err(ctx.pc_apply(b), want) < 1e-13
