@@ -51,15 +51,20 @@ WORKLOADS = {
                newton_steps=3,
                label="256x256 periodic Q3 simple wave (gamma=3, alpha=45deg), HDG condensed, FP64"),
 }
+# run to T = 0.2, FP64 and mixed precision, accuracy and
+# conservation of the mixed path against the FP64 path (the FP64 oracle).
+C3_ACCURACY = dict(nx=256, ny=256, k=3, alpha=45.0, form="hdg", precond="block-jacobi", cfl=1.0, end=0.2,
+                   label="256x256 periodic Q3 simple wave (gamma=3, alpha=45deg), HDG condensed, SSP-DIRK3 "
+                         "CFL 1 to T=0.2, Newton to tol 1e-12, FP64 and mixed precision")
 METRIC = "mean s per accepted Newton update"
 K_NAMES = ["residual", "dg_apply", "dg_jacobi", "condense", "schur_apply", "recover",
            "recovered_residual", "schur_jacobi", "pc_apply", "krylov", "freeze", "admissible", "vector"]
 
 
 # DRAM bytes (read + write) per cell of one launch, from one ncu capture of the
-# kernel on a 64x64 mesh of the same degree (profiles/condense_gj_q4_64x64.txt,
+# kernel on a 64x64 mesh of the same degree (profiles/condense_gj2_q4_64x64.txt,
 # profiles/panel_gemv_q4_64x64.txt); per-launch traffic grows with the cell count.
-NCU_TRAFFIC_PER_CELL = {("condense", 4): 444.54e6 / 4096, ("schur_apply", 4): 216.24e6 / 4096}
+NCU_TRAFFIC_PER_CELL = {("condense", 4): 512.70e6 / 4096, ("schur_apply", 4): 216.24e6 / 4096}
 
 
 def traffic(name, w):
@@ -153,7 +158,7 @@ def ref_binary():
     return None
 
 
-def run_reference_updates(w, newton_steps: int, timeout: float = 900.0):
+def run_reference_updates(w, newton_steps: int, timeout: float = 900.0, integrator: str = "ssp-dirk3"):
     """Run the reference CLI on the first SSP-DIRK3 step of the workload with
     `newton_steps` updates per stage, single-threaded on one core. Returns the
     per-update iteration_s list (the reference's own update timer)."""
@@ -168,7 +173,8 @@ def run_reference_updates(w, newton_steps: int, timeout: float = 900.0):
         cmd = [str(exe), "--nx", str(w["nx"]), "--ny", str(w["ny"]), "--k", str(w["k"]),
                "--alpha-deg", str(w["alpha"]), "--cfl", str(w["cfl"]), "--steps", "1",
                "--newton-steps", str(newton_steps), "--form", w["form"], "--precond", w["precond"],
-               "--assembly", "partial", "--no-save-solution", "--output", str(prefix)]
+               "--assembly", "partial", "--integrator", integrator, "--no-save-solution", "--output",
+               str(prefix)]
         if shutil.which("taskset"):
             cmd = ["taskset", "-c", "0"] + cmd
         proc = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
@@ -177,6 +183,64 @@ def run_reference_updates(w, newton_steps: int, timeout: float = 900.0):
         with open(f"{prefix}_{w['form']}_iterations.csv", newline="") as fh:
             times = [float(r["iteration_s"]) for r in csv.DictReader(fh)]
     return times, exe.name
+
+
+def run_to_time(w, precision, local):
+    """The whole time loop of the workload (eg_run): Newton to the reference's
+    tolerance in every stage, to T = w['end']. Returns the run result."""
+    from mfem_euler2d_cpp_b200 import capi
+
+    ctx = make_context(w, w["form"], local, precision=precision)
+    ro, keep = capi.run_options(integrator="ssp-dirk3", steps=-1, newton_steps=-1, cfl=w["cfl"], end=w["end"],
+                                form_name=w["form"], precond_name=w["precond"])
+    res = capi.RunResult()
+    # the time loop prints the reference's one-line summary on stdout; keep
+    # this process's stdout to the single JSON line
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        t0 = time.perf_counter()
+        rc = ctx.lib.eg_run(ctx.h, capi.C.byref(ro), capi.C.byref(res))
+        wall = time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    ctx._check(rc)
+    ctx.close()
+    del keep
+    return res, wall
+
+
+def c3_accuracy(local, cpu: bool):
+    """FP64 and mixed-precision runs to T = 0.2; final L2
+    errors and conservation drift of both, and the mixed path's error against
+    the FP64 path's (the FP64 oracle). cpu: also the reference's CPU cost of
+    one Newton update on the same mesh (backward Euler, one update)."""
+    w = C3_ACCURACY
+    out = {"workload": w["label"]}
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        res, wall = run_to_time(w, prec, local)
+        runs[prec] = res
+        out[prec] = {"updates": res.updates, "time_steps": res.time_steps, "final_time": res.final_time,
+                     "l2_errors": list(res.errors), "conservation_drift": res.drift,
+                     "mean_newton_device_s": res.newton_device_ms * 1e-3 / max(res.updates, 1),
+                     "time_loop_s": wall}
+    e64 = np.sqrt(np.sum(np.square(runs["fp64"].errors)))
+    emx = np.sqrt(np.sum(np.square(runs["mixed"].errors)))
+    out["joint_l2_error"] = {"fp64": e64, "mixed": emx, "mixed_vs_fp64_relative": abs(emx - e64) / e64}
+    out["within_1pct_of_fp64"] = bool(abs(emx - e64) <= 0.01 * e64)
+    out["mixed_speedup_per_update"] = (out["fp64"]["mean_newton_device_s"] /
+                                       max(out["mixed"]["mean_newton_device_s"], 1e-30))
+    if cpu:
+        times, src = run_reference_updates(dict(w, newton_steps=1), 1, integrator="be")
+        out["cpu_reference_per_update_s"] = float(np.mean(times)) if times else None
+        out["cpu_reference_sample"] = ("one backward-Euler Newton update on the same mesh, degree and CFL "
+                                       f"(the same update algorithm), {src}, one core") if times else src
+    return out
 
 
 def cpu_model():
@@ -444,6 +508,31 @@ def run_ours(args, world, rank, local):
             ach = alg[name][1] / avg_s / 1e9
             hbm_lines[name] = {"achieved_gbs": ach, "frac": ach / peaks["hbm_gbs"], "avg_launch_ms": avg_s * 1e3,
                                "launches": n_op, "traffic": traffic(name, w)}
+    # the dense-contraction classes against the FP64 DGEMM of this GPU
+    tensor_lines = {}
+    for name in ("condense", "dg_jacobi"):
+        if name == "condense":
+            ms, cnt = prof["condense"]
+            launches_ = cnt // 2
+        else:
+            ms = (dg or {}).get("kernel_ms_per_update", {}).get("dg_jacobi")
+            launches_ = None
+        if name == "condense" and launches_:
+            if fp64_peak is None:
+                fp64_peak = fp64_gemm_peak()
+            avg_s = ms * 1e-3 / launches_
+            ach = alg["condense"][1] / avg_s / 1e12
+            tensor_lines["condense"] = {"achieved_tflops": ach, "frac": ach / fp64_peak, "avg_launch_ms": avg_s * 1e3,
+                                        "algorithmic_flops": alg["condense"][1],
+                                        "peak_tflops": fp64_peak, "peak_source": "measured FP64 DGEMM, this GPU"}
+        elif name == "dg_jacobi" and ms:
+            if fp64_peak is None:
+                fp64_peak = fp64_gemm_peak()
+            # one factor per DG update (the reference's n 2/3 m^3 LU count)
+            ach = alg["dg_jacobi"][1] / (ms * 1e-3) / 1e12
+            tensor_lines["dg_jacobi"] = {"achieved_tflops": ach, "frac": ach / fp64_peak, "ms_per_update": ms,
+                                         "algorithmic_flops": alg["dg_jacobi"][1], "peak_tflops": fp64_peak}
+    c3 = None if args.no_c3 else c3_accuracy(local, cpu=(world == 1 and not args.no_cpu_baseline))
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         times, src = run_reference_updates(w, 1)
@@ -482,6 +571,7 @@ def run_ours(args, world, rank, local):
                         "returned, eg_stepper_next, eg_download(U) back into it"},
         "roofline": roofline,
         "hbm_kernels": hbm_lines,
+        "tensor_kernels": tensor_lines,
         "profiled_updates": KP,
         "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]},
         "kernel_ms_per_update": {k: round(v[0] / KP, 3) for k, v in prof.items() if v[1]},
@@ -493,6 +583,7 @@ def run_ours(args, world, rank, local):
         "dg": dg,
         "ilu": ilu,
         "mixed": mixed,
+        "c3_accuracy": c3,
     }
     return line
 
@@ -540,6 +631,7 @@ def main():
     ap.add_argument("--no-ilu", action="store_true", help="skip the secondary block-ILU(0) measurement")
     ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c3", action="store_true", help="skip the 256x256 Q3 run to T=0.2 (FP64 and mixed)")
     ap.add_argument("--ref-max-updates", type=int, default=12)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
