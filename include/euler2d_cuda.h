@@ -202,7 +202,8 @@ long long eg_device_bytes(const eg_ctx *ctx);
 int eg_upload(eg_ctx *ctx, int slot, const double *src);
 int eg_download(eg_ctx *ctx, int slot, double *dst);
 /* Replaces: Problem::Initial (src/problem.cpp:329), L2 projection of the exact
- * wave at t=0 into EG_SLOT_U (host computation, uploaded). */
+ * wave at t=0 into EG_SLOT_U, computed on the device (order max(24, 2k+8)
+ * Gauss-Legendre rule, EulerGas::exact src/physics.cpp:64). */
 int eg_initial(eg_ctx *ctx);
 
 /* ---------------------------------------------------- operators (parity) */
@@ -259,12 +260,17 @@ int eg_newton_residual(eg_ctx *ctx, double *residual_norm);
 int eg_newton_update(eg_ctx *ctx, double residual_norm, double old_norm, eg_update_stats *st);
 
 /* --------------------------------------------------------- diagnostics */
-/* Replaces: Problem::Integral (src/problem.cpp:727) of EG_SLOT_U. */
+/* Replaces: Problem::Integral (src/problem.cpp:727) of EG_SLOT_U (device). */
 int eg_integral(eg_ctx *ctx, double out[4]);
-/* Replaces: Problem::Errors (src/problem.cpp:704) of EG_SLOT_U at time t. */
+/* Replaces: Problem::Errors (src/problem.cpp:704) of EG_SLOT_U at time t
+ * (device; EG_ERR_STEP_INTERVAL for t outside the exact wave's interval). */
 int eg_errors(eg_ctx *ctx, double time, double out[4]);
+/* Replaces: Problem::Differences (src/problem.cpp:739) of EG_SLOT_U and v, a
+ * host or device body vector (device computation). */
+int eg_state_differences(eg_ctx *ctx, const double *v, double out[4]);
 /* Replaces: Problem::Differences (src/problem.cpp:739): L2 norms of u - v per
- * component for two host body vectors of the described problem. */
+ * component for two host body vectors of the described problem, on the host
+ * (no context needed; eg_state_differences is the device form). */
 int eg_differences(const eg_desc *d, const double *u, const double *v, double out[4]);
 
 /* ------------------------------------------------------------ time loop */

@@ -186,6 +186,7 @@ def load() -> C.CDLL:
         "eg_integral": (C.c_int, [vp, _DP]),
         "eg_errors": (C.c_int, [vp, C.c_double, _DP]),
         "eg_differences": (C.c_int, [C.POINTER(Desc), _DP, _DP, _DP]),
+        "eg_state_differences": (C.c_int, [vp, _DP, _DP]),
         "eg_run": (C.c_int, [vp, C.POINTER(RunOpts), C.POINTER(RunResult)]),
         "eg_stepper_create": (C.c_int, [vp, C.POINTER(RunOpts), C.POINTER(vp)]),
         "eg_stepper_next": (C.c_int, [vp, C.POINTER(UpdateStats)]),

@@ -737,9 +737,7 @@ int eg_initial(eg_ctx *ctx) {
   if (!ctx) return EG_ERR_INVALID;
   return guard(ctx, [&] {
     Ctx &c = ctx->c;
-    std::vector<double> u;
-    eg::host::initial(c.desc, u);
-    eg::upload_vec(c, c.u, u.data(), c.nu);
+    eg::field_initial(c, c.u);
     c.residual_ready = false;
     c.sync();
   });
@@ -954,20 +952,23 @@ int eg_newton_update(eg_ctx *ctx, double residual_norm, double old_norm, eg_upda
 int eg_integral(eg_ctx *ctx, double out[4]) {
   if (!ctx || !out) return EG_ERR_INVALID;
   return guard(ctx, [&] {
-    Ctx &c = ctx->c;
-    std::vector<double> u(c.nu);
-    eg::download_vec(c, u.data(), c.u, c.nu);
-    eg::host::integral(c.desc, u.data(), out);
+    eg::field_integral(ctx->c, ctx->c.u, out);
   });
 }
 
 int eg_errors(eg_ctx *ctx, double time, double out[4]) {
   if (!ctx || !out) return EG_ERR_INVALID;
   return guard(ctx, [&] {
+    eg::field_errors(ctx->c, ctx->c.u, time, out);
+  });
+}
+
+int eg_state_differences(eg_ctx *ctx, const double *v, double out[4]) {
+  if (!ctx || !v || !out) return EG_ERR_INVALID;
+  return guard(ctx, [&] {
     Ctx &c = ctx->c;
-    std::vector<double> u(c.nu);
-    eg::download_vec(c, u.data(), c.u, c.nu);
-    eg::host::errors(c.desc, u.data(), time, out);
+    eg::upload_vec(c, c.tmp_body, v, c.nu);
+    eg::field_differences(c, c.u, c.tmp_body, out);
   });
 }
 

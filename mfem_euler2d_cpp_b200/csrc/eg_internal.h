@@ -210,6 +210,7 @@ struct Ctx {
   // error word (derr[0]) and admissibility flag (derr[1])
   int *derr = nullptr;
   double *dscal = nullptr;
+  double *field_partial = nullptr;  // per-cell partials of the diagnostics (4n) and their sum (4)
   double *hscal = nullptr;  // pinned mirror of dscal
   int *herr = nullptr;      // pinned
   // events for per-update device timing
@@ -282,6 +283,15 @@ void launch_transpose_blocks(Ctx &c, double *a, int nblocks, int bs);
 // ---- eg_api.cu ----
 // Sets the context's description (geometry, tables, metrics) for its size.
 void upload_desc(Ctx &c, const eg_desc &d);
+// ---- initial projection and diagnostics (eg_field.cu) ----
+// u <- L2 projection of the exact wave at t = 0 (Problem::Initial).
+void field_initial(Ctx &c, double *u);
+// L2 errors against the exact wave at `time` (Problem::Errors), conserved
+// integrals (Problem::Integral) and L2 norms of u - v (Problem::Differences)
+// of device body vectors; each synchronises the stream and returns on the host.
+void field_errors(Ctx &c, const double *u, double time, double out[4]);
+void field_integral(Ctx &c, const double *u, double out[4]);
+void field_differences(Ctx &c, const double *u, const double *v, double out[4]);
 // ---- block ILU(0) (eg_ilu.cu) ----
 // Fill (and with factor set, factor) the ILU of `form` at the current state /
 // condensation; x = ILU^{-1} b.

@@ -79,14 +79,12 @@ struct Stepper {
       *v = c.step_bufs + (size_t)(slot++) * c.nu;
       EG_CUDA(cudaMemsetAsync(*v, 0, sizeof(double) * c.nu, c.stream));
     }
-    std::vector<double> u;
-    host::initial(c.desc, u);
-    EG_CUDA(cudaMemcpyAsync(c.u, u.data(), sizeof(double) * c.nu, cudaMemcpyHostToDevice, c.stream));
+    field_initial(c, c.u);  // Problem::Initial on the device
     launch_admissible(c, c.u);
     EG_CUDA(cudaMemcpyAsync(c.herr + 1, c.derr + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
     if (!c.herr[1]) fail(EG_ERR_INITIAL, "Initial projection not positive; refine mesh");
-    host::integral(c.desc, u.data(), initial_integral);
+    field_integral(c, c.u, initial_integral);
     stage_count = ro.integrator == 1 ? 1 : 4;
     final_step = time >= ro.end;
     if (keep_stepping())
@@ -277,12 +275,10 @@ int eg_stepper_finish(eg_stepper *s, eg_run_result *res) {
     eg_run_result out{};
     out.final_time = st.time;
     out.time_steps = st.step;
-    std::vector<double> u(c.nu);
-    EG_CUDA(cudaMemcpyAsync(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    eg::host::errors(c.desc, u.data(), st.time, out.errors);
+    // errors and integrals on the device: the state stays resident
+    eg::field_errors(c, c.u, st.time, out.errors);
     double fin[4];
-    eg::host::integral(c.desc, u.data(), fin);
+    eg::field_integral(c, c.u, fin);
     for (int k = 0; k < 4; ++k) out.drift = std::max(out.drift, std::abs(fin[k] - st.initial_integral[k]));
     *res = out;
   });
@@ -332,14 +328,14 @@ int eg_run(eg_ctx *ctx, const eg_run_opts *ro, eg_run_result *res) {
     out.seconds = eg::wall_s() - begin;
     out.final_time = s.time;
     out.time_steps = s.step;
-    std::vector<double> u(c.nu);
-    EG_CUDA(cudaMemcpyAsync(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost, c.stream));
-    c.sync();
-    eg::host::errors(c.desc, u.data(), s.time, out.errors);
+    eg::field_errors(c, c.u, s.time, out.errors);
     double fin[4];
-    eg::host::integral(c.desc, u.data(), fin);
+    eg::field_integral(c, c.u, fin);
     for (int k = 0; k < 4; ++k) out.drift = std::max(out.drift, std::abs(fin[k] - s.initial_integral[k]));
     if (ro->save_solution) {
+      std::vector<double> u(c.nu);
+      EG_CUDA(cudaMemcpyAsync(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost, c.stream));
+      c.sync();
       std::ofstream cs(s.prefix + "_coefficients.csv");
       cs << "element,node,rho,rhou,rhov,energy\n" << std::setprecision(17);
       for (int e = 0; e < c.n; ++e)

@@ -11,10 +11,11 @@ stage's first rms, and within 1e-8 of itself where it is above 1e-6 of that
 residual, where either code's rms is rounding noise); dt within 1e-12;
 Krylov counts within two iterations. Final state:
 every 32nd coefficient within 1e-10 relative and the per-component sums of
-squares within 1e-10; L2 errors within 1e-9 relative; conservation drift
-within 1e-13 of the reference's own (1.12e-12 here: with three Newton updates
-per stage the stage residuals stay near 1e-8, so neither code conserves to
-roundoff on this workload).
+squares within 1e-10; L2 errors within 1e-9 relative; conservation drift no
+larger than the reference's own plus 1e-13. The reference reports 1.12e-12
+here, most of it the rounding of its sequential sum of the 409,600 node
+integrals; the device sums per cell and then over cells in a tree, with ~100x
+less rounding (7e-15 on this run).
 """
 import csv
 import json
@@ -72,4 +73,4 @@ def test_headline_workload_update_by_update(path, tmp_path):
     assert s["time_steps"] == rs["time_steps"]
     for name in ("rho_L2", "rhou_L2", "rhov_L2", "energy_L2"):
         assert abs(s[name] - rs[name]) <= 1e-9 * rs[name] + 1e-15
-    assert abs(s["max_conservation_drift"] - rs["max_conservation_drift"]) <= 1e-13
+    assert s["max_conservation_drift"] <= rs["max_conservation_drift"] + 1e-13
