@@ -243,6 +243,41 @@ def c3_accuracy(local, cpu: bool):
     return out
 
 
+def reference_status(nx, k, alpha, steps=3, newton_steps=3, timeout=600.0):
+    """Outcome of the reference command line on one batch instance: (exit
+    code, its last stderr line or "ok")."""
+    exe = ref_binary()
+    if exe is None:
+        return None, "oracle/_ref binaries not built"
+    with tempfile.TemporaryDirectory() as tmp:
+        cmd = [str(exe), "--nx", str(nx), "--ny", str(nx), "--k", str(k), "--alpha-deg", repr(alpha), "--cfl", "1",
+               "--steps", str(steps), "--newton-steps", str(newton_steps), "--form", "hdg", "--timing-only",
+               "--no-save-solution", "--output", str(Path(tmp) / "ref")]
+        proc = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    msg = proc.stderr.strip().splitlines()[-1] if proc.returncode and proc.stderr.strip() else "ok"
+    return proc.returncode, msg
+
+
+def batch_c4(threads: int, cpu: bool):
+    """BASELINE config 4 (64 seeded uneven instances, 3 steps x 3 updates):
+    the batched mixed-precision path against the plain FP64 path one instance
+    at a time; instances that fail here are run through the reference's own
+    command line and its outcome is recorded beside them."""
+    from mfem_euler2d_cpp_b200 import workloads
+
+    out = workloads.run_batch(count=64, seed=0, threads=threads, precision="mixed")
+    cfg = out.pop("config", {})
+    out["instances"] = cfg.get("instances")
+    if cpu:
+        ref = []
+        for i, tpl, status in out["failed_instances"]:
+            rc, msg = reference_status(tpl[0], tpl[2], tpl[3])
+            ref.append({"instance": i, "nx": tpl[0], "k": tpl[2], "status_here": status,
+                        "reference_exit": rc, "reference_message": msg})
+        out["failed_instances_in_the_reference"] = ref
+    return out
+
+
 def cpu_model():
     try:
         for line in Path("/proc/cpuinfo").read_text().splitlines():
@@ -533,6 +568,7 @@ def run_ours(args, world, rank, local):
             tensor_lines["dg_jacobi"] = {"achieved_tflops": ach, "frac": ach / fp64_peak, "ms_per_update": ms,
                                          "algorithmic_flops": alg["dg_jacobi"][1], "peak_tflops": fp64_peak}
     c3 = None if args.no_c3 else c3_accuracy(local, cpu=(world == 1 and not args.no_cpu_baseline))
+    batch = None if args.no_batch else batch_c4(threads=32, cpu=(world == 1 and not args.no_cpu_baseline))
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         times, src = run_reference_updates(w, 1)
@@ -584,6 +620,7 @@ def run_ours(args, world, rank, local):
         "ilu": ilu,
         "mixed": mixed,
         "c3_accuracy": c3,
+        "batch_c4": batch,
     }
     return line
 
@@ -632,6 +669,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c3", action="store_true", help="skip the 256x256 Q3 run to T=0.2 (FP64 and mixed)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch of BASELINE config 4")
     ap.add_argument("--ref-max-updates", type=int, default=12)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

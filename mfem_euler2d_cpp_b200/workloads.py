@@ -1,13 +1,15 @@
 """Many-instance workloads on one GPU, on the engine's batch and request-loop
 entry points (eg_batch_*, eg_server_*).
 
-batch  Uneven instances run together: `count` seeded simple-wave problems
-       (gamma = 3) with nx = ny drawn from {20,24,32,40,48,64}, k uniform in
-       1..6 and alpha uniform in (15, 75) degrees, each advanced 3 SSP-DIRK3
-       steps x 3 Newton updates at CFL 1 (HDG, block Jacobi; mixed precision
-       by default: FP64 residual and refinement, FP32 preconditioner and inner
-       Schur GMRES). Reports accepted Newton updates/s of the concurrent batch
-       and of the same instances advanced one at a time.
+batch  Uneven instances run together: `count` seeded
+       simple-wave problems (gamma = 3) with nx = ny drawn from
+       {8,16,24,32,48,64}, k uniform in 1..6 and alpha uniform in (15, 75)
+       degrees, each advanced 3 SSP-DIRK3 steps x 3 Newton updates at CFL 1
+       (HDG, block Jacobi; mixed precision by default: FP64 residual and
+       refinement, FP32 preconditioner and inner Schur GMRES). Reports
+       accepted Newton updates/s of the concurrent batch, of the plain FP64
+       path one instance at a time and of the batch's precision one at a
+       time, and checks every instance's L2 error against its FP64 run.
 
 serve  A Poisson stream of time-advance requests (exponential inter-arrival
        times at `rate` requests/s): steps uniform in 1..10, nx = ny from
@@ -36,46 +38,71 @@ import numpy as np
 from . import capi
 
 
-def batch_instances(count: int, seed: int):
+# nx = ny uniform over these sizes, k uniform in 1..6
+C4_SIZES = (8, 16, 24, 32, 48, 64)
+
+
+def batch_instances(count: int, seed: int, sizes=C4_SIZES):
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
-        # meshes coarser than 20 x 20 are left out: 3 CFL-1 steps there leave
-        # the smooth interval of the exact wave (status 18) or produce
-        # inadmissible stages (status 20), in the reference as here
-        n = int(rng.choice([20, 24, 32, 40, 48, 64]))
+        n = int(rng.choice(sizes))
         out.append((n, n, int(rng.integers(1, 7)), float(rng.uniform(15.0, 75.0))))
     return out
 
 
-def run_batch(count=64, seed=0, threads=32, precision="mixed", steps=3, newton_steps=3):
-    inst = batch_instances(count, seed)
-    prec = capi.PRECISION_MIXED if precision == "mixed" else capi.PRECISION_FP64
+def _joint(errors):
+    return float(np.sqrt(np.sum(np.square(errors))))
+
+
+def run_batch(count=64, seed=0, threads=32, precision="mixed", steps=3, newton_steps=3, sizes=C4_SIZES):
+    """The instances run concurrently in `precision`, against the plain FP64
+    path one instance at a time (and `precision` one at a time, which
+    separates what concurrency buys from what the precision buys). Every
+    instance that completes in both is checked: its joint L2 error within 1%
+    of the FP64 run's. Instances that fail keep their status."""
+    inst = batch_instances(count, seed, sizes)
     descs = [capi.simple_wave_desc(*t) for t in inst]
-    opts = [capi.default_opts(form=capi.FORM_HDG, precision=prec) for _ in inst]
     ro, keep = capi.run_options(integrator="ssp-dirk3", steps=steps, newton_steps=newton_steps, cfl=1.0,
                                 form_name="hdg")
-    lines = {}
-    for label, nthreads in (("concurrent", threads), ("one_at_a_time", 1)):
+    runs = {}
+    for label, prec_name, nthreads in (("batched", precision, threads), ("fp64_one_at_a_time", "fp64", 1),
+                                       (f"{precision}_one_at_a_time", precision, 1)):
+        prec = capi.PRECISION_MIXED if prec_name == "mixed" else capi.PRECISION_FP64
+        opts = [capi.default_opts(form=capi.FORM_HDG, precision=prec) for _ in inst]
         with capi.Batch(descs, opts) as b:
             st = b.run(ro, threads=nthreads, check=False)
             statuses = [b.result(i)[0] for i in range(count)]
             errors = [list(b.result(i)[1].errors) for i in range(count)]
-        lines[label] = {"seconds": st.seconds, "updates": st.updates, "updates_per_s": st.updates / st.seconds,
-                        "failed": st.failed, "statuses": statuses, "errors": errors}
-    same = lines["concurrent"]["errors"] == lines["one_at_a_time"]["errors"]
+        runs[label] = {"seconds": st.seconds, "updates": st.updates,
+                       "updates_per_s": st.updates / st.seconds if st.seconds > 0 else 0.,
+                       "failed": st.failed, "statuses": statuses, "errors": errors}
+    bat, ref64 = runs["batched"], runs["fp64_one_at_a_time"]
+    same_prec = runs[f"{precision}_one_at_a_time"]
+    checked, worst, within = 0, 0.0, True
+    for i in range(count):
+        if bat["statuses"][i] == 0 and ref64["statuses"][i] == 0:
+            e0, e1 = _joint(ref64["errors"][i]), _joint(bat["errors"][i])
+            rel = abs(e1 - e0) / e0
+            worst = max(worst, rel)
+            within &= rel <= 0.01
+            checked += 1
     return {
         "metric": "accepted Newton updates/s (batched uneven instances)",
-        "value": lines["concurrent"]["updates_per_s"], "unit": "updates/s", "higher_is_better": True,
-        "baseline_one_at_a_time": lines["one_at_a_time"]["updates_per_s"],
-        "speedup": lines["concurrent"]["updates_per_s"] / lines["one_at_a_time"]["updates_per_s"],
-        "seconds": lines["concurrent"]["seconds"], "updates": lines["concurrent"]["updates"],
-        "failed_instances": lines["concurrent"]["failed"],
-        "failed_statuses": sorted({s for s in lines["concurrent"]["statuses"] if s != 0}),
-        "results_identical_alone_and_batched": same,
-        "config": {"workload": "uneven simple-wave instances", "count": count, "seed": seed, "threads": threads,
-                   "precision": precision, "steps": steps, "newton_steps_per_stage": newton_steps,
-                   "instances": inst},
+        "value": bat["updates_per_s"], "unit": "updates/s", "higher_is_better": True,
+        "baseline_fp64_one_at_a_time": ref64["updates_per_s"],
+        "speedup_vs_fp64_one_at_a_time": bat["updates_per_s"] / ref64["updates_per_s"],
+        f"{precision}_one_at_a_time": same_prec["updates_per_s"],
+        "speedup_vs_same_precision_one_at_a_time": bat["updates_per_s"] / same_prec["updates_per_s"],
+        "seconds": bat["seconds"], "updates": bat["updates"],
+        "failed_instances": [(i, inst[i], bat["statuses"][i]) for i in range(count) if bat["statuses"][i] != 0],
+        "fp64_statuses_of_failed": [ref64["statuses"][i] for i in range(count) if bat["statuses"][i] != 0],
+        "l2_check": {"instances_checked": checked, "worst_relative_difference_vs_fp64": worst,
+                     "all_within_1pct": bool(within)},
+        "results_identical_alone_and_batched": bat["errors"] == same_prec["errors"],
+        "config": {"workload": "BASELINE config 4: uneven seeded simple-wave instances", "count": count,
+                   "seed": seed, "threads": threads, "precision": precision, "steps": steps,
+                   "newton_steps_per_stage": newton_steps, "sizes": list(sizes), "instances": inst},
         "data": "synthetic: seeded simple-wave instances (gamma=3)",
     }
 
