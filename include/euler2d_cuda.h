@@ -272,6 +272,13 @@ int eg_state_differences(eg_ctx *ctx, const double *v, double out[4]);
  * component for two host body vectors of the described problem, on the host
  * (no context needed; eg_state_differences is the device form). */
 int eg_differences(const eg_desc *d, const double *u, const double *v, double out[4]);
+/* Replaces: Problem::Save (src/problem.cpp:762-790) for a host body vector u:
+ * writes prefix.mesh (MFEM mesh v1.0 text of the Cartesian quadrilateral
+ * mesh), prefix_{rho,rhou,rhov,energy}.gf (one L2 Gauss-Legendre grid
+ * function per component) and prefix_coefficients.csv. Host only; no context
+ * needed. EG_ERR_INVALID (message in eg_last_error(NULL)) when a file cannot
+ * be opened. */
+int eg_save_solution(const eg_desc *d, const double *u, const char *prefix);
 
 /* ------------------------------------------------------------ time loop */
 /* Run options: the time-loop subset of euler::Options. */

@@ -186,6 +186,7 @@ def load() -> C.CDLL:
         "eg_integral": (C.c_int, [vp, _DP]),
         "eg_errors": (C.c_int, [vp, C.c_double, _DP]),
         "eg_differences": (C.c_int, [C.POINTER(Desc), _DP, _DP, _DP]),
+        "eg_save_solution": (C.c_int, [C.POINTER(Desc), _DP, C.c_char_p]),
         "eg_state_differences": (C.c_int, [vp, _DP, _DP]),
         "eg_run": (C.c_int, [vp, C.POINTER(RunOpts), C.POINTER(RunResult)]),
         "eg_stepper_create": (C.c_int, [vp, C.POINTER(RunOpts), C.POINTER(vp)]),
@@ -226,6 +227,19 @@ def simple_wave_desc(nx: int, ny: int, k: int, alpha_deg: float, gamma: float = 
     if rc != OK:
         raise EngineError(rc, "invalid simple-wave description")
     return d
+
+
+def save_solution(desc: Desc, u: np.ndarray, prefix: str) -> None:
+    """Problem::Save (src/problem.cpp:762-790) of a host body vector: prefix.mesh,
+    prefix_{rho,rhou,rhov,energy}.gf and prefix_coefficients.csv."""
+    lib = load()
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    q = desc.k + 1
+    if u.size != 4 * q * q * desc.nx * desc.ny:
+        raise EngineError(1, "body vector size does not match the description")
+    rc = lib.eg_save_solution(C.byref(desc), _ptr(u), str(prefix).encode())
+    if rc != OK:
+        raise EngineError(rc, lib.eg_last_error(None).decode())
 
 
 def default_opts(**kw) -> Opts:

@@ -1021,4 +1021,19 @@ int eg_differences(const eg_desc *d, const double *u, const double *v, double ou
   return EG_OK;
 }
 
+int eg_save_solution(const eg_desc *d, const double *u, const char *prefix) {
+  if (!d || !u || !prefix || d->k < 0 || d->k > 8 || d->nx < 2 || d->ny < 2 || !(d->lx > 0) ||
+      !(d->ly > 0))
+    return EG_ERR_INVALID;
+  try {
+    if (!eg::host::save_solution(*d, u, prefix)) {
+      g_create_error = "Cannot open solution output";
+      return EG_ERR_INVALID;
+    }
+  } catch (const std::exception &) {
+    return EG_ERR_INVALID;
+  }
+  return EG_OK;
+}
+
 }  // extern "C"

@@ -336,14 +336,8 @@ int eg_run(eg_ctx *ctx, const eg_run_opts *ro, eg_run_result *res) {
       std::vector<double> u(c.nu);
       EG_CUDA(cudaMemcpyAsync(u.data(), c.u, sizeof(double) * c.nu, cudaMemcpyDeviceToHost, c.stream));
       c.sync();
-      std::ofstream cs(s.prefix + "_coefficients.csv");
-      cs << "element,node,rho,rhou,rhov,energy\n" << std::setprecision(17);
-      for (int e = 0; e < c.n; ++e)
-        for (int i = 0; i < c.p; ++i) {
-          cs << e << ',' << i;
-          for (int k = 0; k < 4; ++k) cs << ',' << u[(size_t)e * c.m + 4 * i + k];
-          cs << '\n';
-        }
+      if (!eg::host::save_solution(c.desc, u.data(), s.prefix))
+        eg::fail(EG_ERR_INVALID, "Cannot open solution output");
     }
     std::ofstream summary(s.prefix + "_summary.csv");
     if (!summary) eg::fail(EG_ERR_INVALID, "Cannot open summary output");

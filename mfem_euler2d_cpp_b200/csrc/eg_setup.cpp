@@ -7,6 +7,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <fstream>
+#include <iomanip>
 #include <stdexcept>
 
 namespace eg {
@@ -274,6 +276,61 @@ void differences(const eg_desc &d, const double *u, const double *v, double out[
         a[c] += d.area * r.w[qp] * diff * diff;
       }
   for (int c = 0; c < 4; ++c) out[c] = std::sqrt(a[c]);
+}
+
+// The mesh is the reference's MakeCartesian2D(nx, ny, QUADRILATERAL, lx, ly) in row-major order
+// (no space-filling-curve reordering), shifted to the centred box (src/problem.cpp:47-51): vertex
+// (i, j) is i + j (nx + 1) at (lx i / nx - lx / 2, ly j / ny - ly / 2),
+// element (i, j) is i + j nx with its corners counter-clockwise from the lower left, and the
+// boundary segments run bottom (attribute 1), right (2), top (3), left (4), each oriented with the
+// domain on its left. The grid functions hold u[e m + 4 i + c] at DOF e p + i, the element-local
+// numbering of an L2 space (FiniteElementSpace::GetElementDofs).
+bool save_solution(const eg_desc &d, const double *u, const std::string &prefix) {
+  const int nx = d.nx, ny = d.ny, q = d.k + 1, p = q * q, m = 4 * p, n = nx * ny;
+  auto vid = [nx](int i, int j) { return i + j * (nx + 1); };
+  {
+    std::ofstream ms(prefix + ".mesh");
+    if (!ms) return false;
+    ms << "MFEM mesh v1.0\n\n"
+          "#\n# MFEM Geometry Types (see mesh/geom.hpp):\n#\n# POINT       = 0\n"
+          "# SEGMENT     = 1\n# TRIANGLE    = 2\n# SQUARE      = 3\n# TETRAHEDRON = 4\n"
+          "# CUBE        = 5\n# PRISM       = 6\n# PYRAMID     = 7\n#\n\n"
+       << "dimension\n2\n\nelements\n" << n << '\n';
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        ms << "1 3 " << vid(i, j) << ' ' << vid(i + 1, j) << ' ' << vid(i + 1, j + 1) << ' '
+           << vid(i, j + 1) << '\n';
+    ms << "\nboundary\n" << 2 * (nx + ny) << '\n';
+    for (int i = 0; i < nx; ++i) ms << "1 1 " << vid(i + 1, 0) << ' ' << vid(i, 0) << '\n';
+    for (int j = 0; j < ny; ++j) ms << "2 1 " << vid(nx, j + 1) << ' ' << vid(nx, j) << '\n';
+    for (int i = 0; i < nx; ++i) ms << "3 1 " << vid(i, ny) << ' ' << vid(i + 1, ny) << '\n';
+    for (int j = 0; j < ny; ++j) ms << "4 1 " << vid(0, j) << ' ' << vid(0, j + 1) << '\n';
+    ms << "\nvertices\n" << (nx + 1) * (ny + 1) << "\n2\n" << std::setprecision(17);
+    for (int j = 0; j <= ny; ++j)
+      for (int i = 0; i <= nx; ++i)
+        ms << d.lx * i / nx - .5 * d.lx << ' ' << d.ly * j / ny - .5 * d.ly << '\n';
+    if (!ms) return false;
+  }
+  static const char *names[] = {"rho", "rhou", "rhov", "energy"};
+  for (int c = 0; c < 4; ++c) {
+    std::ofstream fs(prefix + "_" + names[c] + ".gf");
+    if (!fs) return false;
+    fs << "FiniteElementSpace\nFiniteElementCollection: L2_2D_P" << d.k
+       << "\nVDim: 1\nOrdering: 0\n\n" << std::setprecision(17);
+    for (int e = 0; e < n; ++e)
+      for (int i = 0; i < p; ++i) fs << u[(size_t)e * m + 4 * i + c] << '\n';
+    if (!fs) return false;
+  }
+  std::ofstream cs(prefix + "_coefficients.csv");
+  if (!cs) return false;
+  cs << "element,node,rho,rhou,rhov,energy\n" << std::setprecision(17);
+  for (int e = 0; e < n; ++e)
+    for (int i = 0; i < p; ++i) {
+      cs << e << ',' << i;
+      for (int c = 0; c < 4; ++c) cs << ',' << u[(size_t)e * m + 4 * i + c];
+      cs << '\n';
+    }
+  return bool(cs);
 }
 
 }  // namespace host

@@ -26,8 +26,12 @@ compiled against the MFEM-subset shim. Two kinds of fixture are written:
   with block Jacobi and block ILU(0), DG with block Jacobi): every
   _iterations.csv row, the summary and a strided sample of the final state.
 
+* solution_*.npz -- the solution files of Problem::Save (src/problem.cpp:762)
+  as the reference command line writes them: the .mesh text, the four .gf
+  texts and the final coefficients, per form.
+
 Usage:  python tests/golden/make_golden.py
-            [--only CLI_CASE ... | --trajectories | --condense | --c2 [CASE ...]]
+            [--only CLI_CASE ... | --trajectories | --condense | --c2 [CASE ...] | --solution]
 """
 from __future__ import annotations
 
@@ -291,6 +295,29 @@ def make_cli(exe: Path, name: str, args: list[str]) -> dict:
         return out
 
 
+# a non-square mesh so that vertex, element and boundary numbering are all visible
+SOLUTION_ARGS = ["--nx", "8", "--ny", "6", "--k", "2", "--alpha-deg", "30", "--cfl", "1",
+                 "--steps", "1", "--newton-steps", "2", "--form", "both"]
+GF_NAMES = ("rho", "rhou", "rhov", "energy")
+
+
+def make_solution(exe: Path) -> dict:
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = Path(tmp) / "run"
+        proc = subprocess.run([str(exe), *SOLUTION_ARGS, "--output", str(prefix)],
+                              capture_output=True, text=True)
+        if proc.returncode:
+            raise RuntimeError(f"solution: {proc.stderr}")
+        out = {"args": np.array(json.dumps(SOLUTION_ARGS))}
+        for form in ("dg", "hdg"):
+            out[f"{form}_mesh"] = np.array(Path(f"{prefix}_{form}.mesh").read_text())
+            for name in GF_NAMES:
+                out[f"{form}_{name}_gf"] = np.array(Path(f"{prefix}_{form}_{name}.gf").read_text())
+            coeff = np.loadtxt(f"{prefix}_{form}_coefficients.csv", delimiter=",", skiprows=1)
+            out[f"{form}_u"] = coeff[:, 2:].reshape(-1)
+        return out
+
+
 # (nx, ny, k, alpha_deg): high degrees on meshes with more cells than the
 # condensation launches CTAs (two per SM for k = 5, 6 and one for k = 7, 8 on
 # 148 SMs), so that CTAs reduce several cells each (condense_*.npz)
@@ -431,6 +458,10 @@ def main():
         names = sys.argv[sys.argv.index("--c2") + 1:] or list(C2_CASES)
         make_c2(ref_cli(), names)
         return
+    if "--solution" in sys.argv:  # regenerate just the solution files
+        np.savez_compressed(HERE / "solution_8x6_q2.npz", **make_solution(ref_cli()))
+        print("solution 8x6 q2")
+        return
     if "--condense" in sys.argv:  # regenerate just the high-degree condensation cases
         for i, (nx, ny, k, alpha) in enumerate(CONDENSE_CASES):
             np.savez_compressed(HERE / f"condense_{nx}x{ny}_k{k}.npz",
@@ -470,6 +501,8 @@ def main():
     for i, (nx, ny, k, alpha) in enumerate(CONDENSE_CASES):
         np.savez_compressed(HERE / f"condense_{nx}x{ny}_k{k}.npz", **make_condense(lib, nx, ny, k, alpha, 7000 + i))
         print("condense", nx, ny, k)
+    np.savez_compressed(HERE / "solution_8x6_q2.npz", **make_solution(exe))
+    print("solution 8x6 q2")
     meta = {"iteration_columns": ITER_COLS, "summary_columns": SUMMARY_COLS,
             "unit_cases": UNIT_CASES, "cli_cases": CLI_CASES}
     (HERE / "manifest.json").write_text(json.dumps(meta, indent=1))

@@ -88,3 +88,35 @@ def test_cli_help():
     assert proc.returncode == 0
     assert "--form dg|hdg|both" in proc.stdout
     assert "--assembly full|element|partial" in proc.stdout
+
+
+def _mesh_records(text):
+    """Non-comment, non-blank lines of an MFEM mesh v1.0 text."""
+    return [ln.split() for ln in text.splitlines() if ln.strip() and not ln.startswith("#")]
+
+
+def test_save_solution_writes_reference_files(tmp_path):
+    """Problem::Save (src/problem.cpp:762-790) of the reference's final states:
+    the mesh records, and the .gf and _coefficients.csv texts, equal the
+    reference command line's files byte for byte (the mesh may add MFEM's
+    geometry-type comment block)."""
+    f = np.load(ROOT / "tests" / "golden" / "solution_8x6_q2.npz")
+    d = capi.simple_wave_desc(8, 6, 2, 30.0)
+    for form in ("dg", "hdg"):
+        prefix = tmp_path / form
+        capi.save_solution(d, f[f"{form}_u"], str(prefix))
+        mesh = (tmp_path / f"{form}.mesh").read_text()
+        assert mesh.startswith("MFEM mesh v1.0\n")
+        assert _mesh_records(mesh) == _mesh_records(str(f[f"{form}_mesh"]))
+        for name in ("rho", "rhou", "rhov", "energy"):
+            assert (tmp_path / f"{form}_{name}.gf").read_text() == str(f[f"{form}_{name}_gf"])
+        coeff = np.loadtxt(tmp_path / f"{form}_coefficients.csv", delimiter=",", skiprows=1)
+        np.testing.assert_array_equal(coeff[:, 2:].reshape(-1), f[f"{form}_u"])
+
+
+def test_save_solution_rejects_bad_input(tmp_path):
+    d = capi.simple_wave_desc(8, 6, 2, 30.0)
+    with pytest.raises(capi.EngineError):
+        capi.save_solution(d, np.zeros(7), str(tmp_path / "x"))
+    with pytest.raises(capi.EngineError, match="Cannot open solution output"):
+        capi.save_solution(d, np.zeros(4 * 9 * 48), str(tmp_path / "missing" / "x"))

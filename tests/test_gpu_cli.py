@@ -115,3 +115,22 @@ def test_code_test_assertions(tmp_path):
         comp = next(csv.DictReader(fh))
     assert float(comp["max_nodal_difference"]) < 1e-8
     assert float(comp["solution_L2_difference"]) < 1e-8
+
+
+def test_cli_writes_reference_solution_files(tmp_path):
+    """The --device cuda run writes Problem::Save's files (src/problem.cpp:762-790):
+    the same mesh records as the reference command line, and grid functions
+    whose values equal the reference's final state to 1e-10 relative."""
+    f = np.load(ROOT / "tests" / "golden" / "solution_8x6_q2.npz")
+    prefix = run_cli(json.loads(str(f["args"])), tmp_path)
+    records = lambda t: [ln.split() for ln in t.splitlines() if ln.strip() and not ln.startswith("#")]
+    for form in ("dg", "hdg"):
+        assert records(open(f"{prefix}_{form}.mesh").read()) == records(str(f[f"{form}_mesh"]))
+        for name in ("rho", "rhou", "rhov", "energy"):
+            text = open(f"{prefix}_{form}_{name}.gf").read()
+            ref = str(f[f"{form}_{name}_gf"])
+            head, ref_head = text.split("\n\n")[0], ref.split("\n\n")[0]
+            assert head == ref_head
+            vals = np.array(text.split("\n\n", 1)[1].split(), float)
+            ref_vals = np.array(ref.split("\n\n", 1)[1].split(), float)
+            assert rel_err(vals, ref_vals) < 1e-10
