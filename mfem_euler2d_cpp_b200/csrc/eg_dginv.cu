@@ -195,17 +195,18 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
 }
 
 // The two-phase form of the same inverse (eg_gj.cuh gj2_reduce/gj2_replay):
-// phase 1 reduces the block in shared memory with two CTAs per SM, phase 2
-// replays the recorded panels on the identity, 64 columns per pass. The
+// phase 1 reduces the block in shared memory (two or three CTAs of 8 warps
+// per SM for k = 3, 4; one CTA of 16 warps for k = 5), phase 2 replays the
+// recorded panels on the identity, 16 WC columns per pass. The
 // result W has its rows in pivot order -- row w holds row perm[w] of the
 // inverse -- and is stored column-major as it leaves the registers; the
 // apply scatters through perm.
-template <int Q, int MINB>
-__global__ void __launch_bounds__(256, MINB)
+template <int Q, int MINB, int WR_ = 2, int WC_ = 4>
+__global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
     dg_inverse_gj2_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
                           double *__restrict__ inv, int *__restrict__ perm, int *err) {
   constexpr int M = 4 * Q * Q;
-  using C = Gj2Cfg<M, M>;
+  using C = Gj2Cfg<M, M, WR_, WC_>;
   constexpr int WR = C::WR, WC = C::WC, TRW = C::TRW, NPAN = C::NPAN, KR = C::KR, NP = C::NP, LDA = C::LDA;
   constexpr int TCB = 2, CBW = 8 * TCB * WC, NPASS = (M + CBW - 1) / CBW;
   __shared__ STab<Q> st;
@@ -350,10 +351,10 @@ void launch_inverse(Ctx &c, const double *u) {
   EG_CUDA(cudaGetLastError());
 }
 
-template <int Q, int MINB>
+template <int Q, int MINB, int WR = 2, int WC = 4>
 void launch_inverse2(Ctx &c, const double *u) {
-  using C = Gj2Cfg<4 * Q * Q, 4 * Q * Q>;
-  auto kern = dg_inverse_gj2_kernel<Q, MINB>;
+  using C = Gj2Cfg<4 * Q * Q, 4 * Q * Q, WR, WC>;
+  auto kern = dg_inverse_gj2_kernel<Q, MINB, WR, WC>;
   EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
   const int grid = std::min(c.n, sm_count_dginv() * MINB);
   kern<<<grid, C::THREADS, C::DYN, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, c.pc_dg,
@@ -363,7 +364,7 @@ void launch_inverse2(Ctx &c, const double *u) {
 
 }  // namespace
 
-bool dg_inverse_supported(int q) { return q >= 1 && q <= 5; }
+bool dg_inverse_supported(int q) { return q >= 1 && q <= 6; }
 bool dg_inverse_permuted(int q) { return q >= 4; }
 
 void launch_dg_inverse(Ctx &c, const double *u) {
@@ -375,7 +376,8 @@ void launch_dg_inverse(Ctx &c, const double *u) {
     case 3: launch_inverse<3, 2, 2, 2>(c, u); break;
     case 4: launch_inverse2<4, 3>(c, u); break;
     case 5: launch_inverse2<5, 2>(c, u); break;
-    default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 4");
+    case 6: launch_inverse2<6, 1, 4, 4>(c, u); break;
+    default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 5");
   }
 }
 
@@ -389,7 +391,8 @@ void launch_dg_inverse_apply(Ctx &c, const double *b, double *x) {
     case 3: block_inverse_cm_apply_kernel<36><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
     case 4: block_inverse_cm_apply_kernel<64><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
     case 5: block_inverse_cm_apply_kernel<100><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 4");
+    case 6: block_inverse_cm_apply_kernel<144><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
+    default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 5");
   }
   EG_CUDA(cudaGetLastError());
 }

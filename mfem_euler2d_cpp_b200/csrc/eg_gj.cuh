@@ -171,9 +171,10 @@ __device__ __forceinline__ bool gj_select_pivots(int jbase, double (*pan)[4], do
 // runs fraction-free: the column searched at step s is p w - w_s pw over the
 // previous step's values (scaled by the earlier pivots, which orders the rows
 // as the eliminated column does), so no reciprocal sits on the chain. One
-// warp max-reduction per step on a packed key (25 magnitude bits of the
-// IEEE pattern and 127 - row, so ties go to the first row; magnitudes within
-// 2^-13 of each other count as ties, a choice as stable as the exact one);
+// warp max-reduction per step on a packed key (the top magnitude bits of the
+// IEEE pattern and RMAX - row, so ties go to the first row; with 7 row bits
+// (M <= 128) magnitudes within 2^-13 of each other count as ties, with 8 bits
+// (M <= 256) within 2^-12, a choice as stable as the exact one);
 // the pivot row reaches every lane through shared memory (rowbuf). Writes the
 // pivot rows (pivs), marks them used and records their unknown index (invp);
 // returns false for a zero column (singular cell; the remaining pivots are
@@ -181,6 +182,9 @@ __device__ __forceinline__ bool gj_select_pivots(int jbase, double (*pan)[4], do
 template <int M, int KR, int LDA>
 __device__ __forceinline__ bool gj_pick_pivots(int jbase, const double *Acol, double (*rowbuf)[4], int *pivs,
                                                unsigned char *used, int *invp, int lane) {
+  static_assert(M <= 256, "pivot key holds at most 8 row bits");
+  constexpr int RB = M <= 128 ? 7 : 8;
+  constexpr unsigned RMAX = (1u << RB) - 1u;
   double w[KR][4];
   bool un[KR];
 #pragma unroll
@@ -199,12 +203,12 @@ __device__ __forceinline__ bool gj_pick_pivots(int jbase, const double *Acol, do
     for (int k = 0; k < KR; ++k) {
       const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(w[k][jj]) >> 32) & 0x7fffffffu;
       const unsigned pk =
-          (un[k] && hi <= 0x7ff00000u) ? (((hi >> 7) << 7) | (unsigned)(127 - (lane + 32 * k))) : 0u;
+          (un[k] && hi <= 0x7ff00000u) ? (((hi >> RB) << RB) | (RMAX - (unsigned)(lane + 32 * k))) : 0u;
       best = pk > best ? pk : best;
     }
     const unsigned mb = __reduce_max_sync(0xffffffffu, best);
-    int bi = 127 - (int)(mb & 127u);
-    if ((mb >> 7) == 0u) {
+    int bi = (int)(RMAX - (mb & RMAX));
+    if ((mb >> RB) == 0u) {
       ok = false;
       int cand = 0x7fffffff;
 #pragma unroll
@@ -288,15 +292,16 @@ __device__ __forceinline__ void gj_pivot_block_inverse(double *Acol, const int *
 }
 
 // Shapes of the two-phase Gauss-Jordan for an M x M cell matrix and NR
-// right-hand sides (8 warps: 2 x 4 over 8x8 tiles).
-template <int M_, int NR_>
+// right-hand sides (WR x WC warps over 8x8 tiles: 2 x 4 when two or three
+// CTAs share an SM, 4 x 4 when one CTA fills it).
+template <int M_, int NR_, int WR_ = 2, int WC_ = 4>
 struct Gj2Cfg {
   static constexpr int M = M_, NR = NR_;
   static constexpr int MT = (M + 7) / 8;  // 8x8 tiles per side of A
   // stride of A: LDA % 8 in {2, 6} makes a warp's tile loads conflict-free
   static constexpr int LDA = ((M + 2) % 8 == 6 || (M + 2) % 8 == 2) ? M + 2 : ((M + 6) / 8) * 8 + 6;
   static constexpr int NRT = (NR + 7) / 8;
-  static constexpr int WR = 2, WC = 4, THREADS = 32 * WR * WC;
+  static constexpr int WR = WR_, WC = WC_, THREADS = 32 * WR * WC;
   static constexpr int TRW = (MT + WR - 1) / WR;   // row tiles per warp
   static constexpr int TCA = (MT + WC - 1) / WC;   // A column tiles per warp
   static constexpr int TCW = (NRT + WC - 1) / WC;  // right-hand-side column tiles per warp

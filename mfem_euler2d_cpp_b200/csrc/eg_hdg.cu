@@ -433,12 +433,13 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
   }
 }
 
-// ------------------------------------- two-phase condensation (k <= 4)
+// ------------------------------------- two-phase condensation (k = 3..5)
 // The cell system [A | B | r_e] of the register-resident kernel above fills
 // an SM's register file, so one cell's serial pivot chain leaves the SM idle
-// most of the time. This kernel splits the elimination so that two cells
-// share an SM (two CTAs of 8 warps, at most 128 registers per thread, one
-// copy of A per CTA in shared memory):
+// most of the time. This kernel splits the elimination so that two or three
+// cells share an SM at k = 3, 4 (CTAs of 8 warps, at most 128 registers per
+// thread, one copy of A per CTA in shared memory); at k = 5 A takes 164 KB
+// and one CTA of 16 warps fills the SM:
 //  1. Gauss-Jordan on A alone, in shared memory, in 4-column panels: warp 0
 //     picks the panel's pivots (gj_pick_pivots) and forms T^{-1}
 //     (gj_pivot_block_inverse) while the other warps copy the pivot rows'
@@ -452,14 +453,14 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
 //     overwrites with [X | y]): per panel the pivot rows are published and
 //     one MMA per tile applies the same update. No search runs in this phase.
 // The arithmetic is the register kernel's (the same pivots up to ties
-// within 2^-13, the same panel updates), so the results agree with the
+// within 2^-13, 2^-12 at k = 5, the same panel updates), so the results agree with the
 // reference's LU solve (src/condensation.cpp:131-148) to rounding.
-template <int Q, int MINB>
-__global__ void __launch_bounds__(256, MINB)
+template <int Q, int MINB, int WR_ = 2, int WC_ = 4>
+__global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
     condense_gj2_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
                         const double *__restrict__ r, double *XY, double *Cb, double *sf_out, double *contrib,
                         double *panels, int *err) {
-  using C = Gj2Cfg<4 * Q * Q, 16 * Q + 1>;
+  using C = Gj2Cfg<4 * Q * Q, 16 * Q + 1, WR_, WC_>;
   constexpr int M = C::M, NR = C::NR, WR = C::WR, WC = C::WC;
   constexpr int TRW = C::TRW, TCW = C::TCW, NPAN = C::NPAN, KR = C::KR;
   constexpr int NP = C::NP, NQ = C::NQ, LDA = C::LDA;
@@ -534,9 +535,9 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
-// ------------------------------------------- condensation for k >= 5 (DMMA)
+// ------------------------------------------- condensation for k >= 6 (DMMA)
 // The cell system [A | B | r_e] (m x (m + 4t + 1)) does not fit on chip for
-// k >= 5, so it lives in a per-CTA slab of global memory (L2-resident) and is
+// k >= 6, so it lives in a per-CTA slab of global memory (L2-resident) and is
 // reduced by blocked Gauss-Jordan with virtual partial pivoting in panels of
 // GjgCfg::NB columns:
 //  1. the panel's columns are staged in shared memory and its pivots chosen
@@ -558,7 +559,7 @@ struct GjgCfg {
   static constexpr int RU = 6;                       // row tiles per load round of the update
   static constexpr size_t SMEM = sizeof(double) * ((size_t)2 * NB * M + (size_t)NB * NC + 2 * NB * NB) +
                                  sizeof(int) * (size_t)(3 * M + NB);
-  // two CTAs per SM where their shared memory fits (k = 5, 6): one CTA's
+  // two CTAs per SM where their shared memory fits (k = 6): one CTA's
   // serial pivot chain then overlaps the other's trailing update
   static constexpr int MINB =
       2 * (SMEM + sizeof(CondenseShared<Q>) + 2048) <= 227 * 1024 ? 2 : 1;
@@ -1117,10 +1118,10 @@ static void launch_condense_gj(Ctx &c, const double *u, const double *r) {
                                             c.XY, c.Cb, c.sf, c.contrib, c.panels, c.derr);
 }
 
-template <int Q, int MINB>
+template <int Q, int MINB, int WR = 2, int WC = 4>
 static void launch_condense_gj2(Ctx &c, const double *u, const double *r) {
-  using C = Gj2Cfg<4 * Q * Q, 16 * Q + 1>;
-  auto kern = condense_gj2_kernel<Q, MINB>;
+  using C = Gj2Cfg<4 * Q * Q, 16 * Q + 1, WR, WC>;
+  auto kern = condense_gj2_kernel<Q, MINB, WR, WC>;
   EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
   const int grid = std::min(c.n, sm_count_hdg() * MINB);
   kern<<<grid, C::THREADS, C::DYN, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, r,
@@ -1153,7 +1154,7 @@ void launch_condense(Ctx &c, const double *u, const double *r) {
     case 3: launch_condense_gj<3, 2, 2, 4>(c, u, r); break;
     case 4: launch_condense_gj2<4, 3>(c, u, r); break;
     case 5: launch_condense_gj2<5, 2>(c, u, r); break;
-    case 6: launch_condense_gjg<6>(c, u, r); break;
+    case 6: launch_condense_gj2<6, 1, 4, 4>(c, u, r); break;
     case 7: launch_condense_gjg<7>(c, u, r); break;
     case 8: launch_condense_gjg<8>(c, u, r); break;
     case 9: launch_condense_gjg<9>(c, u, r); break;

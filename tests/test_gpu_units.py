@@ -260,7 +260,7 @@ def test_high_degree_condensation_on_many_cells(condense_case, precision):
         assert rel_err(ctx.recover(lam), f["du"]) < OP_TOL
 
 
-@pytest.mark.parametrize("nx,ny,k", [(12, 10, 1), (10, 8, 2), (6, 5, 3), (5, 6, 4)])
+@pytest.mark.parametrize("nx,ny,k", [(12, 10, 1), (10, 8, 2), (6, 5, 3), (5, 6, 4), (4, 5, 5), (14, 12, 5)])
 def test_dg_pc_blocks_are_inverses(nx, ny, k):
     """After eg_pc_factor(1) the DG block-Jacobi slot holds each cell block's
     explicit inverse, column-major (the k >= 3 factor keeps its rows in pivot
