@@ -699,20 +699,10 @@ int eg_download(eg_ctx *ctx, int slot, double *dst) {
     if (slot == EG_SLOT_PC_BLOCKS) {
       if (c.opts.form == EG_FORM_DG) {
         if (!c.pc_dg) eg::fail(EG_ERR_INVALID, "no preconditioner built");
-        if (c.dg_pc_inverse && eg::dg_inverse_permuted(c.q)) {
-          // stored rows are in pivot order (row w is row perm[w]); the slot
-          // holds the inverse itself, column-major
+        if (eg::dg_pc_is_record(c)) {
+          // the slot holds the inverses the record applies, column-major
           if (!dst) eg::fail(EG_ERR_INVALID, "null vector");
-          const size_t mm = (size_t)c.m * c.m;
-          std::vector<double> w((size_t)c.n * mm);
-          std::vector<int> perm((size_t)c.n * c.m);
-          eg::download_vec(c, w.data(), c.pc_dg, w.size());
-          EG_CUDA(cudaMemcpyAsync(perm.data(), c.piv_dg, sizeof(int) * perm.size(), cudaMemcpyDeviceToHost, c.stream));
-          c.sync();
-          for (int e = 0; e < c.n; ++e)
-            for (int col = 0; col < c.m; ++col)
-              for (int row = 0; row < c.m; ++row)
-                dst[e * mm + (size_t)col * c.m + perm[(size_t)e * c.m + row]] = w[e * mm + (size_t)col * c.m + row];
+          eg::download_dg_record_inverse(c, dst);
         } else {
           eg::download_vec(c, dst, c.pc_dg, (size_t)c.n * c.m * c.m);
         }

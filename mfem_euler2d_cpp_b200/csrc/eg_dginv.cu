@@ -1,25 +1,27 @@
-// DG block Jacobi as explicit inverses (PartialDGOperator::DiagonalBlocks,
-// src/partial.cpp:265-298, factored as in src/linear.cpp:198-202 and applied
-// by LinearSolver::Impl::Precondition, src/linear.cpp:66-75).
+// DG block Jacobi (PartialDGOperator::DiagonalBlocks, src/partial.cpp:265-298,
+// factored as in src/linear.cpp:198-202 and applied by
+// LinearSolver::Impl::Precondition, src/linear.cpp:66-75) without triangular
+// sweeps. Both forms below pick the pivots LUFactors::Factor would choose
+// (virtual row partial pivoting, eg_gj.cuh) and use the FP64 tensor cores.
 //
-// Factor: each cell's m x m diagonal block is built at the Newton state and
-// inverted in place by the blocked Gauss-Jordan of the HDG condensation
-// (eg_gj.cuh): 4-column panels, virtual row partial pivoting (the pivots
-// LUFactors::Factor would choose), one m8n8k4 FP64 MMA per 8x8 tile and
-// panel. In place means the panel's columns, once eliminated, take the unit
-// columns e_{pivot row} of the identity the inverse is built from, so every
-// panel updates every tile (2 m^3 flops per block instead of the LU's
-// 2/3 m^3) and nothing beyond the block is held on chip. The inverse is
-// written column-major.
+// k <= 2 -- explicit inverses: each cell's m x m block is inverted in place
+// by a register-resident Gauss-Jordan (the panel's columns, once eliminated,
+// take the unit columns of the identity the inverse is built from: 2 m^3
+// flops), written column-major and applied as a column-major block GEMV,
+// one warp per cell, lanes over rows, 16-byte loads.
 //
-// Apply: x_e = A_e^{-1} b_e as a column-major block GEMV, one warp per cell,
-// lanes over rows: every load of the inverse is a contiguous 16-byte access
-// per lane, so the apply streams the n m^2 doubles once at HBM speed where
-// the triangular sweeps of an LU apply are latency bound.
+// k = 3..5 -- Gauss-Jordan records: phase 1 of the two-phase Gauss-Jordan
+// (gj2_reduce: A in shared memory, 4-column panels, m^3 flops) and nothing
+// more; the reduced block, the panels' T^{-1} and their pivot rows leave the
+// SM as the record. The apply replays the elimination on the right-hand
+// side, panel by panel, one warp per cell: it streams the m^2 doubles of the
+// record once, the traffic of an explicit inverse, while the factor skips
+// the 2 m^3 flops of replaying the elimination on the identity.
 #include <algorithm>
 
 #include "eg_cellmat.cuh"
 #include "eg_gj.cuh"
+#include "eg_bulk.cuh"
 #include "eg_internal.h"
 
 namespace eg {
@@ -194,90 +196,6 @@ __global__ void __launch_bounds__(32 * WR *WC, MINB)
   }
 }
 
-// The two-phase form of the same inverse (eg_gj.cuh gj2_reduce/gj2_replay):
-// phase 1 reduces the block in shared memory (two or three CTAs of 8 warps
-// per SM for k = 3, 4; one CTA of 16 warps for k = 5), phase 2 replays the
-// recorded panels on the identity, 16 WC columns per pass. The
-// result W has its rows in pivot order -- row w holds row perm[w] of the
-// inverse -- and is stored column-major as it leaves the registers; the
-// apply scatters through perm.
-template <int Q, int MINB, int WR_ = 2, int WC_ = 4>
-__global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
-    dg_inverse_gj2_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
-                          double *__restrict__ inv, int *__restrict__ perm, int *err) {
-  constexpr int M = 4 * Q * Q;
-  using C = Gj2Cfg<M, M, WR_, WC_>;
-  constexpr int WR = C::WR, WC = C::WC, TRW = C::TRW, NPAN = C::NPAN, KR = C::KR, NP = C::NP, LDA = C::LDA;
-  constexpr int TCB = 2, CBW = 8 * TCB * WC, NPASS = (M + CBW - 1) / CBW;
-  __shared__ STab<Q> st;
-  __shared__ double us[M], UT[16 * Q], FM[4 * Q * 16];
-  __shared__ double topA[4][NP];
-  __shared__ double topR[2][4][CBW];
-  __shared__ double rowbuf[KR * 32][4];
-  __shared__ double fac[NPAN][16];
-  __shared__ int pivs[NPAN][4];
-  __shared__ int invp[KR * 32];
-  __shared__ unsigned char used[KR * 32];
-  __shared__ int sing;
-  extern __shared__ __align__(16) double A[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wr = warp % WR, wc = warp / WR;
-  const int gq = lane >> 2, tq = lane & 3;
-  load_tables<Q>(st, tab);
-  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < M; i += C::THREADS) us[i] = u[(size_t)e * M + i];
-    __syncthreads();
-    cell_traces<Q>(st, us, UT);
-    __syncthreads();
-    dg_face_matrices<Q>(UT, FM, g, fz, e);
-    __syncthreads();
-    build_cell_matrix<Q>(A, LDA, st, us, FM, g);
-    for (int i = threadIdx.x; i < KR * 32; i += C::THREADS) {
-      used[i] = i >= M ? 1 : 0;
-      invp[i] = 0;
-    }
-    if (threadIdx.x == 0) sing = 0;
-    __syncthreads();
-    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing);
-    double *W = inv + (size_t)e * M * M;
-#pragma unroll 1
-    for (int pass = 0; pass < NPASS; ++pass) {
-      const int c0 = pass * CBW;
-      double acc[TRW][TCB][2];
-#pragma unroll
-      for (int a = 0; a < TRW; ++a) {
-        const int row = (wr + a * WR) * 8 + gq;
-#pragma unroll
-        for (int b = 0; b < TCB; ++b) {
-          const int col = c0 + (wc + b * WC) * 8 + 2 * tq;
-          acc[a][b][0] = (row < M && col == row) ? 1. : 0.;
-          acc[a][b][1] = (row < M && col + 1 == row) ? 1. : 0.;
-        }
-      }
-      gj2_replay<C, TCB>(A, fac, pivs, topR, acc);
-#pragma unroll
-      for (int a = 0; a < TRW; ++a) {
-        const int row = (wr + a * WR) * 8 + gq;
-        if (row < M) {
-#pragma unroll
-          for (int b = 0; b < TCB; ++b) {
-            const int col = c0 + (wc + b * WC) * 8 + 2 * tq;
-            if (col < M) W[(size_t)col * M + row] = acc[a][b][0];
-            if (col + 1 < M) W[(size_t)(col + 1) * M + row] = acc[a][b][1];
-          }
-        }
-      }
-      __syncthreads();  // topR is reused by the next pass
-    }
-    if (sing) {
-      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_JACOBI);
-      continue;
-    }
-    for (int i = threadIdx.x; i < M; i += C::THREADS) perm[(size_t)e * M + i] = invp[i];
-  }
-}
-
 // x_e = A_e^{-1} b_e, inverses column-major: one warp per cell, lane l holds
 // rows 2l, 2l+1 (+ 64 s); the right-hand side is staged per warp in shared
 // memory and broadcast column by column.
@@ -328,6 +246,180 @@ __global__ void __launch_bounds__(256) block_inverse_cm_apply_kernel(const doubl
   }
 }
 
+// ------------------------------------------------ Gauss-Jordan record (k = 3..5)
+// Factor without the identity replay: phase 1 of the two-phase Gauss-Jordan
+// (gj2_reduce) on the cell block, then its record leaves the SM as it is --
+// the m x m reduced block column-major (the panel columns hold the
+// eliminated entries, T_r - e_r on the pivot rows), T^{-1} of every panel
+// (fac: NPAN x 16, row-major 4x4) and the panels' pivot rows (pivs) -- with
+// the unknown order invp of the result rows (perm). The record holds as
+// many bytes as an explicit inverse, so the apply streams the same traffic,
+// but the factor does m^3 flops instead of the inverse's 3 m^3.
+template <int Q, int MINB, int WR_ = 2, int WC_ = 4>
+__global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
+    dg_gj_record_kernel(Geo g, const double *__restrict__ tab, Frozen fz, const double *__restrict__ u,
+                        double *__restrict__ rec, double *__restrict__ rec_fac, int *__restrict__ rec_pivs,
+                        int *__restrict__ perm, int *err) {
+  constexpr int M = 4 * Q * Q;
+  using C = Gj2Cfg<M, M, WR_, WC_>;
+  constexpr int NPAN = C::NPAN, KR = C::KR, NP = C::NP, LDA = C::LDA;
+  __shared__ STab<Q> st;
+  __shared__ double us[M], UT[16 * Q], FM[4 * Q * 16];
+  __shared__ double topA[4][NP];
+  __shared__ double rowbuf[KR * 32][4];
+  __shared__ double fac[NPAN][16];
+  __shared__ int pivs[NPAN][4];
+  __shared__ int invp[KR * 32];
+  __shared__ unsigned char used[KR * 32];
+  __shared__ int sing;
+  extern __shared__ __align__(16) double A[];
+  load_tables<Q>(st, tab);
+  for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < M; i += C::THREADS) us[i] = u[(size_t)e * M + i];
+    __syncthreads();
+    cell_traces<Q>(st, us, UT);
+    __syncthreads();
+    dg_face_matrices<Q>(UT, FM, g, fz, e);
+    __syncthreads();
+    build_cell_matrix<Q>(A, LDA, st, us, FM, g);
+    for (int i = threadIdx.x; i < KR * 32; i += C::THREADS) {
+      used[i] = i >= M ? 1 : 0;
+      invp[i] = 0;
+    }
+    if (threadIdx.x == 0) sing = 0;
+    __syncthreads();
+    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing);
+    if (sing) {
+      if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_JACOBI);
+      continue;
+    }
+    double *R = rec + (size_t)e * M * M;
+    for (int i = threadIdx.x; i < M * M; i += C::THREADS) R[i] = A[(i % M) + (size_t)(i / M) * LDA];
+    for (int i = threadIdx.x; i < NPAN * 16; i += C::THREADS) rec_fac[(size_t)e * NPAN * 16 + i] = fac[i >> 4][i & 15];
+    for (int i = threadIdx.x; i < M; i += C::THREADS) {
+      rec_pivs[(size_t)e * M + i] = pivs[i >> 2][i & 3];
+      perm[(size_t)e * M + i] = invp[i];
+    }
+  }
+}
+
+// Shapes of the record apply: NB panel buffers per warp, W warps (cells) per
+// CTA, sized so that two CTAs share an SM where they fit.
+template <int M>
+struct RecApplyCfg {
+  static constexpr int NPAN = M / 4;
+  static constexpr int NB = 3;                      // panels in flight per warp
+  static constexpr int W = M <= 100 ? 8 : 4;        // warps (cells) per CTA
+  static constexpr int PANEL = 4 * M;               // doubles per panel (contiguous in the record)
+  static constexpr int PIVS = (M + 3) / 4 * 4;      // ints, padded to 16 bytes
+  // per warp: NB panel buffers, the panels' T^{-1}, the pivot rows
+  static constexpr size_t WARP_BYTES = sizeof(double) * ((size_t)NB * PANEL + (size_t)NPAN * 16) + sizeof(int) * PIVS;
+  static constexpr size_t DYN = WARP_BYTES * W;
+};
+
+// x_e = A_e^{-1} b_e from the Gauss-Jordan record: one warp per cell, lane l
+// holds rows l + 32 s of the working vector. Per panel p (in order) the
+// pivot rows' values reach every lane by shuffles, t = T_p^{-1} x[pivots],
+// and every row takes x_i -= a_i . t with a_i its four panel entries (on a
+// pivot row T_r - e_r, which leaves t there): the replay of the elimination
+// on one right-hand side. The record reaches shared memory by bulk copies
+// (a panel's four columns are one contiguous run of the column-major
+// record), NB panels ahead of the replay, each buffer completed on its own
+// mbarrier; the panels' T^{-1} and pivot rows arrive with the first panel.
+// The record streams once, as an explicit inverse would. The result is in
+// pivot order (row w is unknown perm[w]) and is scattered on the way out.
+// Waits are bounded: a copy that does not land within kRecSpinLimit polls
+// raises DERR_WAIT_LIMIT and the warp returns after a bounded drain.
+constexpr unsigned kRecSpinLimit = 1u << 20;
+template <int M>
+__global__ void __launch_bounds__(32 * RecApplyCfg<M>::W) dg_gj_apply_kernel(
+    const double *__restrict__ rec, const double *__restrict__ rec_fac, const int *__restrict__ rec_pivs,
+    const int *__restrict__ perm, int nblocks, const double *__restrict__ b, double *__restrict__ x,
+    const int *__restrict__ skip, int *err) {
+  using C = RecApplyCfg<M>;
+  constexpr int S = (M + 31) / 32, NPAN = C::NPAN, NB = C::NB, PANEL = C::PANEL;
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ __align__(8) unsigned long long bars[C::W][NB];
+  if (skip != nullptr && *skip) return;  // speculative Arnoldi step after convergence
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int blk = blockIdx.x * C::W + warp;
+  if (blk >= nblocks) return;  // warp-uniform; nothing below synchronises the CTA
+  double *buf = reinterpret_cast<double *>(reinterpret_cast<char *>(dsm) + C::WARP_BYTES * warp);
+  double *Fs = buf + (size_t)NB * PANEL;
+  int *Ps = reinterpret_cast<int *>(Fs + NPAN * 16);
+  const double *R = rec + (size_t)blk * M * M;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NB; ++k) mbar_init(&bars[warp][k]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(&bars[warp][0], (unsigned)(sizeof(double) * (PANEL + NPAN * 16) + sizeof(int) * M));
+    bulk_load(Fs, rec_fac + (size_t)blk * NPAN * 16, (unsigned)(sizeof(double) * NPAN * 16), &bars[warp][0]);
+    bulk_load(Ps, rec_pivs + (size_t)blk * M, (unsigned)(sizeof(int) * M), &bars[warp][0]);
+    bulk_load(buf, R, (unsigned)(sizeof(double) * PANEL), &bars[warp][0]);
+#pragma unroll
+    for (int k = 1; k < NB; ++k)
+      if (k < NPAN) {
+        mbar_expect(&bars[warp][k], (unsigned)(sizeof(double) * PANEL));
+        bulk_load(buf + (size_t)k * PANEL, R + (size_t)k * PANEL, (unsigned)(sizeof(double) * PANEL), &bars[warp][k]);
+      }
+  }
+  __syncwarp();
+  double v[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int i = lane + 32 * s;
+    v[s] = i < M ? b[(size_t)blk * M + i] : 0.;
+  }
+#pragma unroll 1
+  for (int p = 0; p < NPAN; ++p) {
+    const int k = p % NB;
+    const unsigned parity = (unsigned)((p / NB) & 1);
+    if (!mbar_wait(&bars[warp][k], parity, kRecSpinLimit)) {
+      if (lane == 0) raise_err(err, DERR_WAIT_LIMIT);
+      // let the copies already issued land before the warp leaves
+      for (int q = p; q < NPAN && q < p + NB; ++q)
+        mbar_wait(&bars[warp][q % NB], (unsigned)((q / NB) & 1), kRecSpinLimit);
+      return;
+    }
+    const double *pan = buf + (size_t)k * PANEL;
+    double xp[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int pr = Ps[4 * p + r];
+      double sel = 0.;
+#pragma unroll
+      for (int s = 0; s < S; ++s)
+        if ((pr >> 5) == s) sel = v[s];
+      xp[r] = __shfl_sync(0xffffffffu, sel, pr & 31);
+    }
+    const double *F = Fs + 16 * p;
+    double t[4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+      t[kk] = F[4 * kk] * xp[0] + F[4 * kk + 1] * xp[1] + F[4 * kk + 2] * xp[2] + F[4 * kk + 3] * xp[3];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int i = lane + 32 * s;
+      if (i < M) v[s] -= pan[i] * t[0] + pan[M + i] * t[1] + pan[2 * M + i] * t[2] + pan[3 * M + i] * t[3];
+    }
+    __syncwarp();  // every lane has read buffer k before it is refilled
+    if (lane == 0 && p + NB < NPAN) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect(&bars[warp][k], (unsigned)(sizeof(double) * PANEL));
+      bulk_load(buf + (size_t)k * PANEL, R + (size_t)(p + NB) * PANEL, (unsigned)(sizeof(double) * PANEL),
+                &bars[warp][k]);
+    }
+  }
+  const int *pb = perm + (size_t)blk * M;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int i = lane + 32 * s;
+    if (i < M) x[(size_t)blk * M + pb[i]] = v[s];
+  }
+}
+
 int sm_count_dginv() {
   static int n = 0;
   if (!n) {
@@ -352,20 +444,54 @@ void launch_inverse(Ctx &c, const double *u) {
 }
 
 template <int Q, int MINB, int WR = 2, int WC = 4>
-void launch_inverse2(Ctx &c, const double *u) {
-  using C = Gj2Cfg<4 * Q * Q, 4 * Q * Q, WR, WC>;
-  auto kern = dg_inverse_gj2_kernel<Q, MINB, WR, WC>;
+void launch_record(Ctx &c, const double *u) {
+  constexpr int M = 4 * Q * Q;
+  using C = Gj2Cfg<M, M, WR, WC>;
+  if (!c.dg_rec_fac) {
+    c.dg_rec_fac = c.alloc_n<double>((size_t)c.n * (M / 4) * 16);
+    c.dg_rec_pivs = c.alloc_n<int>((size_t)c.n * M);
+  }
+  auto kern = dg_gj_record_kernel<Q, MINB, WR, WC>;
   EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
   const int grid = std::min(c.n, sm_count_dginv() * MINB);
   kern<<<grid, C::THREADS, C::DYN, c.stream>>>(c.geo, c.tab, Frozen{c.fa, c.fbb, c.flw, c.frw, c.fpen}, u, c.pc_dg,
-                                                c.piv_dg, c.derr);
+                                                c.dg_rec_fac, c.dg_rec_pivs, c.piv_dg, c.derr);
   EG_CUDA(cudaGetLastError());
+}
+
+template <int M>
+void launch_record_apply(Ctx &c, const double *b, double *x, const int *skip) {
+  using C = RecApplyCfg<M>;
+  auto kern = dg_gj_apply_kernel<M>;
+  EG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::DYN));
+  kern<<<(c.n + C::W - 1) / C::W, 32 * C::W, C::DYN, c.stream>>>(c.pc_dg, c.dg_rec_fac, c.dg_rec_pivs, c.piv_dg,
+                                                                   c.n, b, x, skip, c.derr);
+}
+
+void record_apply(Ctx &c, const double *b, double *x, const int *skip) {
+  switch (c.q) {
+    case 4: launch_record_apply<64>(c, b, x, skip); break;
+    case 5: launch_record_apply<100>(c, b, x, skip); break;
+    case 6: launch_record_apply<144>(c, b, x, skip); break;
+    default: fail(EG_ERR_INVALID, "Gauss-Jordan records cover k = 3..5");
+  }
+  EG_CUDA(cudaGetLastError());
+}
+
+// b = e_col in every cell; inv[e][col][:] = x_e (column col of the cell's inverse)
+__global__ void unit_column_kernel(long long n, int M, int col, double *b) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n * M; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (int)(i % M) == col ? 1. : 0.;
+}
+__global__ void store_column_kernel(long long n, int M, int col, const double *x, double *inv) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n * M; i += (long long)gridDim.x * blockDim.x)
+    inv[(i / M) * M * M + (size_t)col * M + i % M] = x[i];
 }
 
 }  // namespace
 
 bool dg_inverse_supported(int q) { return q >= 1 && q <= 6; }
-bool dg_inverse_permuted(int q) { return q >= 4; }
+bool dg_pc_is_record(const Ctx &c) { return c.dg_pc_inverse && c.q >= 4 && c.q <= 6; }
 
 void launch_dg_inverse(Ctx &c, const double *u) {
   c.ensure_pc_dg();
@@ -374,27 +500,54 @@ void launch_dg_inverse(Ctx &c, const double *u) {
     case 1: launch_inverse<1, 1, 1, 8>(c, u); break;
     case 2: launch_inverse<2, 1, 2, 4>(c, u); break;
     case 3: launch_inverse<3, 2, 2, 2>(c, u); break;
-    case 4: launch_inverse2<4, 3>(c, u); break;
-    case 5: launch_inverse2<5, 2>(c, u); break;
-    case 6: launch_inverse2<6, 1, 4, 4>(c, u); break;
-    default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 5");
+    case 4: launch_record<4, 3>(c, u); break;
+    case 5: launch_record<5, 2>(c, u); break;
+    case 6: launch_record<6, 1, 4, 4>(c, u); break;
+    default: fail(EG_ERR_INVALID, "DG block inverses and records support k <= 5");
   }
 }
 
 void launch_dg_inverse_apply(Ctx &c, const double *b, double *x) {
   ProfScope ps(c, EG_K_PC_APPLY, 1);
+  if (c.q >= 4) {
+    record_apply(c, b, x, c.skip);
+    return;
+  }
   const int grid = (c.n + 7) / 8;
-  const int *perm = dg_inverse_permuted(c.q) ? c.piv_dg : nullptr;
   switch (c.q) {
-    case 1: block_inverse_cm_apply_kernel<4><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    case 2: block_inverse_cm_apply_kernel<16><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    case 3: block_inverse_cm_apply_kernel<36><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    case 4: block_inverse_cm_apply_kernel<64><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    case 5: block_inverse_cm_apply_kernel<100><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    case 6: block_inverse_cm_apply_kernel<144><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, perm); break;
-    default: fail(EG_ERR_INVALID, "explicit DG block inverses support k <= 5");
+    case 1: block_inverse_cm_apply_kernel<4><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, nullptr); break;
+    case 2: block_inverse_cm_apply_kernel<16><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, nullptr); break;
+    case 3: block_inverse_cm_apply_kernel<36><<<grid, 256, 0, c.stream>>>(c.pc_dg, c.n, b, x, c.skip, nullptr); break;
+    default: fail(EG_ERR_INVALID, "explicit DG block inverses cover k <= 2");
   }
   EG_CUDA(cudaGetLastError());
+}
+
+void download_dg_record_inverse(Ctx &c, double *dst) {
+  const long long n = c.n;
+  const int M = c.m;
+  double *b = nullptr, *x = nullptr, *inv = nullptr;
+  const size_t vec = sizeof(double) * (size_t)n * M;
+  if (cudaMalloc(&b, vec) != cudaSuccess || cudaMalloc(&x, vec) != cudaSuccess ||
+      cudaMalloc(&inv, vec * M) != cudaSuccess) {
+    cudaFree(b);
+    cudaFree(x);
+    cudaGetLastError();
+    fail(EG_ERR_OUT_OF_MEMORY, "no device memory to expand the DG block-Jacobi record");
+  }
+  const int grid = (int)std::min<long long>((n * M + 255) / 256, 148LL * 16);
+  for (int col = 0; col < M; ++col) {
+    unit_column_kernel<<<grid, 256, 0, c.stream>>>(n, M, col, b);
+    record_apply(c, b, x, nullptr);
+    store_column_kernel<<<grid, 256, 0, c.stream>>>(n, M, col, x, inv);
+  }
+  EG_CUDA(cudaGetLastError());
+  const cudaError_t e = cudaMemcpyAsync(dst, inv, vec * M, cudaMemcpyDeviceToHost, c.stream);
+  const cudaError_t s = cudaStreamSynchronize(c.stream);
+  cudaFree(b);
+  cudaFree(x);
+  cudaFree(inv);
+  if (e != cudaSuccess || s != cudaSuccess) fail(EG_ERR_CUDA, cudaGetErrorString(e != cudaSuccess ? e : s));
 }
 
 }  // namespace eg

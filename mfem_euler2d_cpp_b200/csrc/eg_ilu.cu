@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "eg_bulk.cuh"
 #include "eg_cellmat.cuh"
 #include "eg_internal.h"
 
@@ -101,40 +102,6 @@ __device__ bool wait_local(const volatile unsigned *count, unsigned target, int 
 // CTA ever publishes, so every wait on another CTA runs out.
 __device__ __forceinline__ unsigned long long need(unsigned long long tag, int slot, int starve) {
   return starve ? ~0ull : (tag | (unsigned long long)(slot + 1));
-}
-
-// mbarrier + bulk copy (cp.async.bulk, this CTA only) into its shared memory.
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes) {
-  asm volatile(
-      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
-      "r"(bytes)
-      : "memory");
-}
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit) {
-  for (unsigned it = 0; it < limit; ++it)
-    if (mbar_try(bar, parity)) return true;
-  return false;
 }
 
 // ------------------------------------------------------------- scheduling

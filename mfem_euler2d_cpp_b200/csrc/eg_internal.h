@@ -191,9 +191,13 @@ struct Ctx {
   double *work_gj = nullptr;    // k >= 5 condensation: one m x (m + 4t + 1) slab per CTA
   int work_gj_slots = 0;
   // preconditioners (factored in place): DG n blocks m x m, HDG nf blocks t x t;
-  // dg_pc_inverse: pc_dg holds explicit inverses (column-major), else pivoted LU
+  // dg_pc_inverse: pc_dg holds explicit inverses (column-major, k <= 2) or a
+  // Gauss-Jordan record (k = 3..5, with dg_rec_fac and dg_rec_pivs), else
+  // pivoted LU
   double *pc_dg = nullptr, *pc_hdg = nullptr;
   bool dg_pc_inverse = false;
+  double *dg_rec_fac = nullptr;
+  int *dg_rec_pivs = nullptr;
   int *piv_dg = nullptr, *piv_hdg = nullptr;
   // Krylov workspace (size N = max(nu, nl) so both forms share it)
   int kN = 0, kR = 0;
@@ -265,11 +269,14 @@ void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblock
 void launch_dg_jacobi_apply(Ctx &c, const double *b, double *x);
 // ---- explicit DG block-Jacobi inverses (eg_dginv.cu) ----
 bool dg_inverse_supported(int q);
-// with q >= 4 the stored inverse has its rows in pivot order: row w is row
-// piv_dg[e*m + w] of the cell's true inverse
-bool dg_inverse_permuted(int q);
-void launch_dg_inverse(Ctx &c, const double *u);  // pc_dg <- column-major J_KK^{-1}
+// k <= 2: pc_dg holds the column-major J_KK^{-1}; k = 3..5: the Gauss-Jordan
+// record (pc_dg: reduced block, dg_rec_fac: panel T^{-1}, dg_rec_pivs: panel
+// pivot rows, piv_dg: unknown order of the result rows)
+bool dg_pc_is_record(const Ctx &c);
+void launch_dg_inverse(Ctx &c, const double *u);
 void launch_dg_inverse_apply(Ctx &c, const double *b, double *x);
+// the explicit inverses a record applies, column-major (n m^2 doubles, host)
+void download_dg_record_inverse(Ctx &c, double *dst);
 // ---- launchers (eg_hdg.cu) ----
 void launch_condense(Ctx &c, const double *u, const double *r);
 void launch_schur_apply(Ctx &c, const double *v, double *y);

@@ -43,6 +43,27 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 
 constexpr int kChunk = 8;  // Krylov columns per register chunk
 
+// Sum of n CTA partials p[0..n) by one warp in a fixed order: lane l adds
+// p[l + 32 i] into four interleaved accumulators (four independent loads in
+// flight instead of one dependent chain), then a warp tree. The order depends
+// on n only, so the result is bitwise reproducible for a given grid.
+__device__ __forceinline__ double warp_sum_partials(const double *__restrict__ p, int n) {
+  const int lane = threadIdx.x & 31;
+  double t0 = 0., t1 = 0., t2 = 0., t3 = 0.;
+  int b = lane;
+  for (; b + 96 < n; b += 128) {
+    t0 += p[b];
+    t1 += p[b + 32];
+    t2 += p[b + 64];
+    t3 += p[b + 96];
+  }
+  for (; b < n; b += 32) t0 += p[b];
+  double t = (t0 + t1) + (t2 + t3);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+  return t;
+}
+
 // ---------------------------------------------------------- weighted norm
 template <class T>
 __global__ void __launch_bounds__(kRedThreads)
@@ -239,12 +260,15 @@ __global__ void __launch_bounds__(kCgsThreads)
   __shared__ double mt[2 * EG_MAX_P];
   __shared__ double pin[NC];
   __shared__ double gst[MODE == 2 ? 3 * (kMaxRestart + 1) : 1];  // Givens staging (norm pass)
-  if (ctl->stop) return;  // speculative Arnoldi step after convergence
+  // the control words, the metric and the projections are independent loads:
+  // issue them together and test for a stopped cycle after (a speculative
+  // Arnoldi step after convergence returns without touching w)
+  const int stop = ctl->stop, j = ctl->j;
   for (int i = threadIdx.x; i < period / 4; i += blockDim.x) mt[i] = mtab[i];
   if (MODE > 0)
     for (int i = threadIdx.x; i < ncols; i += blockDim.x) pin[i] = ctl->proj[i];
+  if (stop) return;
   __syncthreads();
-  const int j = ctl->j;
   double acc[NC];
 #pragma unroll
   for (int k = 0; k < NC; ++k) acc[k] = 0.;
@@ -289,14 +313,10 @@ __global__ void __launch_bounds__(kCgsThreads)
   const int nred = MODE == 2 ? 1 : ncols;
   cta_reduce_columns<NC>(acc, nred, red, partials, gridDim.x);
   if (last_block(counter)) {
-    // one warp per column: each lane adds a fixed stride of the CTA partials
-    // in order, then a warp tree (fixed order: bitwise reproducible)
+    // one warp per column (warp_sum_partials: fixed order, bitwise reproducible)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int c = warp; c < nred; c += kCgsThreads / 32) {
-      double t = 0.;
-      for (int b = lane; b < (int)gridDim.x; b += 32) t += partials[(size_t)c * gridDim.x + b];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+      const double t = warp_sum_partials(partials + (size_t)c * gridDim.x, (int)gridDim.x);
       if (lane == 0) {
         if (MODE == 2) {
           const double next = sqrt(t);
@@ -321,7 +341,8 @@ __global__ void __launch_bounds__(kCgsThreads)
 template <class T>
 __global__ void normalize_kernel(int N, const T *__restrict__ w, T *__restrict__ vnext, const GmresCtl *ctl) {
   const double next = ctl->next;
-  if (!(next > 0) || ctl->stop) return;  // a stopped cycle never reads V_{j+1}
+  const int stop = ctl->stop;
+  if (!(next > 0) || stop) return;  // a stopped cycle never reads V_{j+1}
   const double s = 1. / next;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     vnext[i] = (T)((double)w[i] * s);
