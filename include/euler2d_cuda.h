@@ -96,8 +96,10 @@ enum eg_slot {
   EG_SLOT_Y = 8,       /* HDG particular responses y (nu) */
   EG_SLOT_PC_BLOCKS = 9, /* preconditioner blocks, column-major (count: eg_pc_size).
                           block-jacobi: DG n*m*m, HDG nf*t*t; after eg_pc_factor(ctx, 1) HDG
-                          and DG with k <= 5 hold explicit inverses (DG column-major), DG with
-                          k >= 6 packed pivoted LU.
+                          and DG with k <= 5 hold explicit inverses (DG column-major; for
+                          k = 3..5 the device keeps a Gauss-Jordan record and the
+                          download expands it into the inverses it applies), DG
+                          with k >= 6 packed pivoted LU.
                           block-ilu0: the BSR blocks of the ILU in FixedBlockILU order (rows
                           ascending, block columns ascending); after eg_pc_factor(ctx, 1) the
                           strictly lower blocks hold L, the others U (diagonal unfactored). */
