@@ -174,11 +174,11 @@ struct DgOps : LinearOps {
     mtab = c.mtab_dg;
     period = c.m;
   }
-  // partial assembly: the Jacobian from the state inside every action;
-  // element/full: the assembled cell and face-coupling blocks
+  // partial assembly: the Jacobians cached by the refresh at the start of
+  // the solve; element/full: the assembled cell and face-coupling blocks
   void apply(Ctx &c, const double *x, double *y) override {
     if (c.opts.assembly == EG_ASSEMBLY_PARTIAL)
-      launch_dg_apply(c, c.u, x, y);
+      launch_dg_apply_cached(c, x, y);
     else
       launch_assembled_apply(c, EG_FORM_DG, x, y);
   }
@@ -250,6 +250,10 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
   const bool assembled = form == EG_FORM_DG ? c.opts.assembly != EG_ASSEMBLY_PARTIAL
                                             : c.opts.assembly == EG_ASSEMBLY_FULL;
   double t0 = now_s();
+  // DG partial assembly: PartialDGOperator::Refresh at the Newton state
+  // (src/stepper.cpp:139), kept for the whole solve like the reference's
+  if (form == EG_FORM_DG && c.opts.assembly == EG_ASSEMBLY_PARTIAL && (refresh || !c.dgc_vol))
+    launch_dg_refresh(c, c.u);
   if (refresh && assembled) assemble_blocks(c, form);
   out.assembly = now_s() - t0;
   t0 = now_s();
@@ -798,7 +802,8 @@ int eg_dg_apply(eg_ctx *ctx, const double *x, double *y) {
   return guard(ctx, [&] {
     Ctx &c = ctx->c;
     eg::upload_vec(c, c.tmp_body, x, c.nu);
-    eg::launch_dg_apply(c, c.u, c.tmp_body, c.er);
+    eg::launch_dg_refresh(c, c.u);
+    eg::launch_dg_apply_cached(c, c.tmp_body, c.er);
     eg::download_vec(c, y, c.er, c.nu);
   });
 }

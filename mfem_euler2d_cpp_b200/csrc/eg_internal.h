@@ -198,6 +198,9 @@ struct Ctx {
   bool dg_pc_inverse = false;
   double *dg_rec_fac = nullptr;
   int *dg_rec_pivs = nullptr;
+  // DG partial assembly (launch_dg_refresh): dt w J_x, dt w J_y per cell node
+  // and lw J(U_L) + pen I, rw J(U_R) - pen I per face point, component-major
+  double *dgc_vol = nullptr, *dgc_face = nullptr;
   int *piv_dg = nullptr, *piv_hdg = nullptr;
   // Krylov workspace (size N = max(nu, nl) so both forms share it)
   int kN = 0, kR = 0;
@@ -260,7 +263,10 @@ struct Ctx {
 void launch_freeze(Ctx &c, const double *u, bool check_admissible);
 void launch_admissible(Ctx &c, const double *u);  // writes dscal[DS_ADMISSIBLE]
 void launch_residual(Ctx &c, const double *u, const double *old, double *r);
-void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y);
+void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y);  // Jacobians recomputed
+// PartialDGOperator::Refresh at state u, then the cached action (Mult)
+void launch_dg_refresh(Ctx &c, const double *u);
+void launch_dg_apply_cached(Ctx &c, const double *x, double *y);
 void launch_dg_jacobi(Ctx &c, const double *u, bool factor);
 void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,
                         const double *b, double *x);
