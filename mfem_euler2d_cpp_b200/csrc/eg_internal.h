@@ -201,6 +201,7 @@ struct Ctx {
   // DG partial assembly (launch_dg_refresh): dt w J_x, dt w J_y per cell node
   // and lw J(U_L) + pen I, rw J(U_R) - pen I per face point, component-major
   double *dgc_vol = nullptr, *dgc_face = nullptr;
+  double *dgc_h = nullptr;  // the action's face values, 4 per face point
   int *piv_dg = nullptr, *piv_hdg = nullptr;
   // Krylov workspace (size N = max(nu, nl) so both forms share it)
   int kN = 0, kR = 0;
