@@ -130,6 +130,11 @@ typedef struct eg_desc {
 } eg_desc;
 
 /* Solver options (the numerical subset of euler::Options, include/euler.hpp:46-57). */
+/* Linear solver of the Newton system: restarted GMRES, or the dense direct
+ * LU of the full assembly (--solver dense; --solver direct needs MKL PARDISO,
+ * which neither the reference's portable build nor this library has). */
+enum eg_solver { EG_SOLVER_GMRES = 0, EG_SOLVER_DENSE = 1 };
+
 typedef struct eg_opts {
   int form;        /* eg_form */
   int precond;     /* eg_precond */
@@ -139,6 +144,9 @@ typedef struct eg_opts {
   int max_krylov;  /* GMRES iteration limit (default 1500) */
   double linear_tol; /* default 1e-12 */
   int check_update;  /* HDG: independent DG solve of every update (stepper.cpp:184-201) */
+  int solver;        /* eg_solver (Options::solver, src/options.cpp:56-57, 111-112):
+                        EG_SOLVER_DENSE needs EG_ASSEMBLY_FULL, FP64 and at most 5000
+                        unknowns in the solved system (src/linear.cpp:46-47) */
 } eg_opts;
 
 /* Per-update statistics: the numeric columns of _iterations.csv

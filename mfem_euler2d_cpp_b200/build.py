@@ -23,7 +23,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libeuler2d_cuda.so"
 CLI = PKG / "bin" / "euler2d"
 
-CUDA_SOURCES = ["eg_cell.cu", "eg_hdg.cu", "eg_krylov.cu", "eg_api.cu", "eg_run.cu", "eg_ilu.cu", "eg_mixed.cu", "eg_noalloc.cu", "eg_dginv.cu", "eg_field.cu"]
+CUDA_SOURCES = ["eg_cell.cu", "eg_hdg.cu", "eg_krylov.cu", "eg_api.cu", "eg_run.cu", "eg_ilu.cu", "eg_mixed.cu", "eg_noalloc.cu", "eg_dginv.cu", "eg_field.cu", "eg_dense.cu"]
 CXX_SOURCES = ["eg_setup.cpp", "eg_batch.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -34,6 +34,7 @@ STATUS_NAMES = {
     25: "EG_ERR_CONTEXT_LOST",
 }
 FORM_DG, FORM_HDG = 0, 1
+SOLVER_GMRES, SOLVER_DENSE = 0, 1
 PC_JACOBI, PC_ILU0 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 ASSEMBLY_PARTIAL, ASSEMBLY_FULL, ASSEMBLY_ELEMENT = 0, 1, 2
@@ -65,7 +66,7 @@ class Opts(C.Structure):
     _fields_ = [
         ("form", C.c_int), ("precond", C.c_int), ("assembly", C.c_int), ("precision", C.c_int),
         ("restart", C.c_int), ("max_krylov", C.c_int), ("linear_tol", C.c_double),
-        ("check_update", C.c_int),
+        ("check_update", C.c_int), ("solver", C.c_int),
     ]
 
 

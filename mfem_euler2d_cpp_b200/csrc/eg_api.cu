@@ -257,8 +257,12 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
   if (refresh && assembled) assemble_blocks(c, form);
   out.assembly = now_s() - t0;
   t0 = now_s();
+  const bool dense = c.opts.solver == EG_SOLVER_DENSE;
   if (refresh) {
-    pc_factor(c, form, true);
+    if (dense)
+      dense_factor(c, form);  // src/linear.cpp:204-206 (no preconditioner)
+    else
+      pc_factor(c, form, true);
   }
   out.setup = now_s() - t0;
   t0 = now_s();
@@ -269,7 +273,9 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
                      c.opts.precond == EG_PC_BLOCK_JACOBI;
   double res = 0.;
   try {
-    if (mixed) {
+    if (dense) {
+      dense_solve(c, rhs, x);  // src/linear.cpp:224-225; the residual follows below
+    } else if (mixed) {
       if (refresh) mixed_prepare(c);
       res = schur_refine_mixed(c, rhs, x, refresh, tol, c.opts.max_krylov, rhs_norm, &count);
     } else {
@@ -537,6 +543,8 @@ void eg_opts_default(eg_opts *o) {
   o->restart = 20;
   o->max_krylov = 1500;
   o->linear_tol = 1e-12;
+  o->check_update = 0;
+  o->solver = EG_SOLVER_GMRES;
 }
 
 static void validate_opts(const eg_opts &o) {
@@ -552,6 +560,15 @@ static void validate_opts(const eg_opts &o) {
     eg::fail(EG_ERR_INVALID, "Invalid assembly");
   if (o.precision == EG_PRECISION_MIXED && o.assembly == EG_ASSEMBLY_FULL)
     eg::fail(EG_ERR_INVALID, "mixed precision requires partial or element assembly");
+  if (o.solver != EG_SOLVER_GMRES && o.solver != EG_SOLVER_DENSE) eg::fail(EG_ERR_INVALID, "Invalid solver");
+  if (o.solver == EG_SOLVER_DENSE && o.assembly != EG_ASSEMBLY_FULL)
+    eg::fail(EG_ERR_INVALID, "Direct LU requires --assembly full");
+}
+// LinearSolver workspace (src/linear.cpp:46-47): the dense solve's size limit
+static void validate_dense_size(const Ctx &c) {
+  if (c.opts.solver != EG_SOLVER_DENSE) return;
+  const long long n = c.opts.form == EG_FORM_DG ? (long long)c.nu : (long long)c.nl;
+  if (n > eg::kDenseMaxUnknowns) eg::fail(EG_ERR_INVALID, "Dense direct solve limited to 5000 unknowns");
 }
 
 int eg_create(const eg_desc *d, const eg_opts *o, eg_ctx **out) {
@@ -576,6 +593,7 @@ int eg_create(const eg_desc *d, const eg_opts *o, eg_ctx **out) {
       eg::fail(EG_ERR_INVALID, "Mesh/degree exceeds int DOF capacity");
     c.nu = c.n * c.m;
     c.nl = c.nf * c.t;
+    validate_dense_size(c);
     for (int i = 0; i < c.p; ++i)
       if (d->tensor_node[i] != i)
         eg::fail(EG_ERR_INVALID, "native node order must be lexicographic (x fastest)");
@@ -650,6 +668,7 @@ int eg_set_opts(eg_ctx *ctx, const eg_opts *o) {
     if (o->assembly != ctx->c.opts.assembly)
       eg::fail(EG_ERR_INVALID, "assembly is fixed when the context is created");
     ctx->c.opts = *o;
+    validate_dense_size(ctx->c);
     if (o->form == EG_FORM_HDG) ctx->c.ensure_hdg();
   });
 }

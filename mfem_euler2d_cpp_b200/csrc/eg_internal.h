@@ -202,6 +202,10 @@ struct Ctx {
   // and lw J(U_L) + pen I, rw J(U_R) - pen I per face point, component-major
   double *dgc_vol = nullptr, *dgc_face = nullptr;
   double *dgc_h = nullptr;  // the action's face values, 4 per face point
+  // --solver dense: the assembled system as a column-major N x N LU with its pivots
+  double *dense_a = nullptr;
+  int *dense_piv = nullptr;
+  int dense_n = 0;
   int *piv_dg = nullptr, *piv_hdg = nullptr;
   // Krylov workspace (size N = max(nu, nl) so both forms share it)
   int kN = 0, kR = 0;
@@ -268,6 +272,10 @@ void launch_dg_apply(Ctx &c, const double *u, const double *x, double *y);  // J
 // PartialDGOperator::Refresh at state u, then the cached action (Mult)
 void launch_dg_refresh(Ctx &c, const double *u);
 void launch_dg_apply_cached(Ctx &c, const double *x, double *y);
+// ---- dense direct solve of the full assembly (eg_dense.cu) ----
+constexpr int kDenseMaxUnknowns = 5000;
+void dense_factor(Ctx &c, int form);  // LU of the assembled blocks of c.ilu[form]
+void dense_solve(Ctx &c, const double *b, double *x);
 void launch_dg_jacobi(Ctx &c, const double *u, bool factor);
 void launch_block_apply(Ctx &c, const double *blocks, const int *piv, int nblocks, int bs,
                         const double *b, double *x);

@@ -171,7 +171,8 @@ Options parse(int argc, char **argv) {
   // Device-path scope (the reference binary serves the rest).
   require(o.device == "cuda", "This executable is the --device cuda path; use the reference euler2d for CPU runs");
   require(o.precision == "fp64" || o.precision == "mixed", "Invalid precision");
-  require(o.solver == "gmres", "--solver direct/dense is not available with --device cuda");
+  // --solver direct is MKL PARDISO, which the reference's portable build lacks too
+  require(o.solver != "direct", "--solver direct requires MFEM with MKL PARDISO");
   require(o.precision == "fp64" || o.assembly != "full", "--precision mixed requires --assembly partial or element");
   require(o.ilu_ordering == "none", "--ilu-ordering mdf is not available with --device cuda");
   require(!o.verify, "--verify is a CPU diagnostic of the reference build");
@@ -203,6 +204,7 @@ FormResult run_form(const Options &o, const eg_desc &desc, const std::string &fo
   eo.max_krylov = o.max_krylov;
   eo.linear_tol = o.linear_tol;
   eo.check_update = o.check_update ? 1 : 0;
+  eo.solver = o.solver == "dense" ? EG_SOLVER_DENSE : EG_SOLVER_GMRES;
   eg_ctx *ctx = nullptr;
   check(eg_create(&desc, &eo, &ctx), ctx);
   const std::string prefix = o.output + "_" + form;

@@ -250,6 +250,9 @@ CLI_CASES = {
     "full_ilu_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "30", "--cfl", "1",
                         "--steps", "1", "--newton-steps", "2", "--form", "both", "--assembly", "full",
                         "--precond", "block-ilu0"],
+    # dense direct LU of the full assembly (src/linear.cpp:46-49, 204-206, 224-225)
+    "dense_8x8_q2": ["--nx", "8", "--ny", "8", "--k", "2", "--alpha-deg", "30", "--cfl", "1",
+                     "--steps", "1", "--newton-steps", "2", "--form", "both", "--solver", "dense"],
 }
 ITER_COLS = ["step", "stage", "newton", "time", "dt", "cfl", "residual_physical_rms", "damping",
              "krylov_iterations", "linear_relative_residual", "dg_linear_relative_residual",

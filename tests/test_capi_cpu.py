@@ -75,6 +75,11 @@ def _cli(*args):
     (["--assembly", "csr"], "Invalid assembly"),
     (["--solver", "direct", "--assembly", "element"], "Direct LU requires --assembly full"),
     (["--assembly", "full", "--precision", "mixed"], "--precision mixed requires --assembly partial or element"),
+    # the reference's portable build has no MKL PARDISO either: same message
+    (["--solver", "direct"], "--solver direct requires MFEM with MKL PARDISO"),
+    # LinearSolver workspace limit (src/linear.cpp:46-47), raised before any device work
+    (["--solver", "dense", "--nx", "40", "--ny", "40", "--k", "3", "--form", "dg"],
+     "Dense direct solve limited to 5000 unknowns"),
 ])
 def test_cli_rejects_invalid_options(args, message):
     proc = _cli(*args)
