@@ -237,6 +237,9 @@ static void linear_solve(Ctx &c, int form, const double *rhs, double *x, double 
   HdgOps hdg(c);
   LinearOps &ops = form == EG_FORM_DG ? static_cast<LinearOps &>(dg) : static_cast<LinearOps &>(hdg);
   out = LinearOut();
+  // the residual and work vectors below live in the Krylov workspace, which
+  // the dense solve needs as well
+  c.ensure_krylov();
   const double rhs_norm = wnorm(c, rhs, ops.N, ops.mtab, ops.period);
   out.rhs_norm = rhs_norm;
   if (rhs_norm == 0.) {
