@@ -67,8 +67,14 @@ def test_cli_matches_reference(path, tmp_path):
             assert abs(s[name] - rs[name]) <= 1e-9 * rs[name] + 1e-15
         assert s["max_conservation_drift"] < 1e-13  # the reference's own drift here: 3e-15 to 3.4e-14
         assert summary["device"] == "cuda"
-        assembly = args[args.index("--assembly") + 1] if "--assembly" in args else "partial"
+        # a direct solver defaults to full assembly and no preconditioner (src/options.cpp:136-142)
+        solver = args[args.index("--solver") + 1] if "--solver" in args else "gmres"
+        default_assembly = "partial" if solver == "gmres" else "full"
+        assembly = args[args.index("--assembly") + 1] if "--assembly" in args else default_assembly
         assert summary["assembly"] == assembly
+        assert summary["solver"] == solver
+        if solver != "gmres":
+            assert summary["preconditioner"] == "none"
         assert int(summary["matrix_free"]) == (assembly != "full")  # src/options.cpp:135
     with open(f"{prefix}_comparison.csv", newline="") as fh:
         comp = next(csv.DictReader(fh))
