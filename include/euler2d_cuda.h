@@ -58,9 +58,10 @@ enum eg_status {
   EG_ERR_INITIAL = 21,          /* "Initial projection not positive; refine mesh" stepper.cpp:32 */
   EG_ERR_UPDATE_EQUATION = 22,  /* "Independent recovered DG equation check failed" stepper.cpp:190 */
   EG_ERR_UPDATE_EQUIVALENCE = 23, /* "DG/HDG one-update equivalence failed" stepper.cpp:197 */
-  EG_ERR_WAIT_LIMIT = 24,       /* a bounded device-side wait of a dependency-driven sweep gave up
-                                   (no counterpart in the reference, which runs the sweep serially);
-                                   the context stays usable */
+  EG_ERR_WAIT_LIMIT = 24,       /* a bounded device-side wait gave up: a dependency-driven block
+                                   ILU(0) factor or sweep, or a bulk copy of the DG block-Jacobi
+                                   record apply (no counterpart in the reference, whose factor and
+                                   sweeps are serial); the context stays usable */
   EG_ERR_CONTEXT_LOST = 25,     /* after a wait gave up, a bulk copy of the aborted sweep did not
                                    land within its own bound either: the context's device memory
                                    can no longer be trusted, every later call on it returns this
