@@ -278,6 +278,21 @@ def batch_c4(threads: int, cpu: bool):
     return out
 
 
+def serve_c5():
+    """BASELINE config 5, bounded: 48 requests of its distribution (Poisson
+    arrivals at 200 requests/s, 1..10 SSP-DIRK3 steps, k 2..6, meshes 20^2 to
+    64^2; the full distribution's 128^2 Q7-Q8 requests take minutes each),
+    served by 16 workers in mixed precision against the plain FP64 path one
+    request at a time, with every request's L2 error checked against that
+    run's."""
+    from mfem_euler2d_cpp_b200 import workloads
+
+    out = workloads.run_serve(requests=48, rate=200.0, seed=1, workers=16, budget_gb=120.0, precision="mixed",
+                              max_nx=64, max_k=6)
+    out["config"]["sample"] = "first 48 requests of the seeded stream, nx <= 64, k <= 6"
+    return out
+
+
 def cpu_model():
     try:
         for line in Path("/proc/cpuinfo").read_text().splitlines():
@@ -569,6 +584,7 @@ def run_ours(args, world, rank, local):
                                          "algorithmic_flops": alg["dg_jacobi"][1], "peak_tflops": fp64_peak}
     c3 = None if args.no_c3 else c3_accuracy(local, cpu=(world == 1 and not args.no_cpu_baseline))
     batch = None if args.no_batch else batch_c4(threads=32, cpu=(world == 1 and not args.no_cpu_baseline))
+    serve = None if (args.no_serve or world > 1) else serve_c5()  # one GPU: the request loop's device 0
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         times, src = run_reference_updates(w, 1)
@@ -621,6 +637,7 @@ def run_ours(args, world, rank, local):
         "mixed": mixed,
         "c3_accuracy": c3,
         "batch_c4": batch,
+        "serve_c5": serve,
     }
     return line
 
@@ -670,6 +687,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c3", action="store_true", help="skip the 256x256 Q3 run to T=0.2 (FP64 and mixed)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch of BASELINE config 4")
+    ap.add_argument("--no-serve", action="store_true", help="skip the 48-request serve sample of BASELINE config 5")
     ap.add_argument("--ref-max-updates", type=int, default=12)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -18,8 +18,8 @@ serve  A Poisson stream of time-advance requests (exponential inter-arrival
        the smooth interval of the exact wave (request_cfl). Requests are submitted at their arrival
        times to a request loop with a device-memory budget; reports solves/s
        and p50/p99 latency (finish - arrival), beside the same stream served
-       one request at a time, and checks that every request's L2 errors are
-       identical in both runs.
+       one request at a time by the plain FP64 path, and checks every
+       request's L2 error against that run's (within 1%).
 
     python -m mfem_euler2d_cpp_b200.workloads batch --count 64 --seed 0
     python -m mfem_euler2d_cpp_b200.workloads serve --requests 2000 --rate 200 --seed 1
@@ -156,19 +156,33 @@ def _serve(reqs, workers, budget_bytes, precision):
 
 def run_serve(requests=2000, rate=200.0, seed=1, workers=16, budget_gb=120.0, precision="mixed", max_nx=128,
               max_k=8):
+    """The request stream served by `workers` in `precision`, against the
+    plain FP64 path serving the same stream one request at a time. Every
+    request that completes in both is checked: its joint L2 error within 1%
+    of the FP64 run's."""
     reqs = serve_requests(requests, rate, seed, max_nx, max_k)
     budget = int(budget_gb * (1 << 30))
     served = _serve(reqs, workers, budget, precision)
-    single = _serve(reqs, 1, budget, precision)
-    same = served["errors"] == single["errors"]
+    single = _serve(reqs, 1, budget, "fp64")
+    checked, worst, within = 0, 0.0, True
+    for i in range(len(reqs)):
+        if served["statuses"][i] == 0 and single["statuses"][i] == 0:
+            e0, e1 = _joint(single["errors"][i]), _joint(served["errors"][i])
+            rel = abs(e1 - e0) / e0
+            worst = max(worst, rel)
+            within &= rel <= 0.01
+            checked += 1
     for d in (served, single):
         d.pop("errors")
         d["failed_statuses"] = sorted({s for s in d.pop("statuses") if s != 0})
     return {
         "metric": "solves/s with p50/p99 request latency (served time-advance requests)",
         "value": served["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
-        "p50_s": served["p50_s"], "p99_s": served["p99_s"], "served": served, "one_at_a_time": single,
-        "results_identical_alone_and_in_the_mix": same,
+        "p50_s": served["p50_s"], "p99_s": served["p99_s"], "served": served, "fp64_one_at_a_time": single,
+        "speedup_vs_fp64_one_at_a_time": served["solves_per_s"] / single["solves_per_s"]
+        if single["solves_per_s"] > 0 else None,
+        "l2_check": {"requests_checked": checked, "worst_relative_difference_vs_fp64": worst,
+                     "all_within_1pct": bool(within)},
         "config": {"workload": "Poisson stream of simple-wave time-advance requests", "requests": requests,
                    "rate_per_s": rate, "seed": seed, "workers": workers, "budget_gb": budget_gb,
                    "precision": precision, "max_nx": max_nx, "max_k": max_k, "newton_steps_per_stage": 3},
