@@ -330,8 +330,10 @@ struct RecApplyCfg {
 // The record streams once, as an explicit inverse would. The result is in
 // pivot order (row w is unknown perm[w]) and is scattered on the way out.
 // Waits are bounded: a copy that does not land within kRecSpinLimit polls
-// raises DERR_WAIT_LIMIT and the warp returns after a bounded drain.
+// raises DERR_WAIT_LIMIT and the warp returns after a bounded drain of the
+// copies it issued (EG_ERR_CONTEXT_LOST when even that runs out).
 constexpr unsigned kRecSpinLimit = 1u << 20;
+constexpr unsigned kRecDrainLimit = 1u << 24;  // abort path: let an issued copy land
 template <int M>
 __global__ void __launch_bounds__(32 * RecApplyCfg<M>::W) dg_gj_apply_kernel(
     const double *__restrict__ rec, const double *__restrict__ rec_fac, const int *__restrict__ rec_pivs,
@@ -378,9 +380,13 @@ __global__ void __launch_bounds__(32 * RecApplyCfg<M>::W) dg_gj_apply_kernel(
     const unsigned parity = (unsigned)((p / NB) & 1);
     if (!mbar_wait(&bars[warp][k], parity, kRecSpinLimit)) {
       if (lane == 0) raise_err(err, DERR_WAIT_LIMIT);
-      // let the copies already issued land before the warp leaves
+      // let the copies already issued land before the warp leaves; if even
+      // the longer drain bound runs out, a copy may still write this CTA's
+      // shared memory: err[2] tells the host the context can no longer be
+      // trusted
       for (int q = p; q < NPAN && q < p + NB; ++q)
-        mbar_wait(&bars[warp][q % NB], (unsigned)((q / NB) & 1), kRecSpinLimit);
+        if (!mbar_wait(&bars[warp][q % NB], (unsigned)((q / NB) & 1), kRecDrainLimit) && lane == 0)
+          atomicExch(err + 2, 1);
       return;
     }
     const double *pan = buf + (size_t)k * PANEL;
