@@ -321,9 +321,17 @@ struct Gj2Cfg {
 // (W_i -= a_i T^{-1} W_top, a_i = T_r - e_r on pivot rows), loads first,
 // then MMAs, then stores. The panel columns are never written again:
 // together with fac (T^{-1}) and pivs they record the elimination.
-template <class C>
+// The caller's `side(p, t, nt)` runs on the other warps (thread t of nt)
+// while warp 0 searches panel p's pivots: work that does not touch A (the
+// condensation stages its right-hand sides there), which fills the time
+// those warps would spend waiting at the barrier.
+struct Gj2NoSide {
+  __device__ void operator()(int, int, int) const {}
+};
+template <class C, class Side = Gj2NoSide>
 __device__ __forceinline__ void gj2_reduce(double *A, double (*topA)[C::NP], double (*rowbuf)[4], double (*fac)[16],
-                                           int (*pivs)[4], unsigned char *used, int *invp, int *sing) {
+                                           int (*pivs)[4], unsigned char *used, int *invp, int *sing,
+                                           const Side &side = Side()) {
   constexpr int M = C::M, LDA = C::LDA, WR = C::WR, WC = C::WC, TRW = C::TRW, TCA = C::TCA;
   constexpr int NPAN = C::NPAN, KR = C::KR, NP = C::NP, MT = C::MT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -333,8 +341,11 @@ __device__ __forceinline__ void gj2_reduce(double *A, double (*topA)[C::NP], dou
     for (int p = 0; p < NPAN; ++p) {
       const int j = 4 * p;
       double *Acol = A + (size_t)j * LDA;
-      if (warp == 0 && !gj_pick_pivots<M, KR, LDA>(j, Acol, rowbuf, pivs[p], used, invp, lane) && lane == 0)
-        *sing = 1;
+      if (warp == 0) {
+        if (!gj_pick_pivots<M, KR, LDA>(j, Acol, rowbuf, pivs[p], used, invp, lane) && lane == 0) *sing = 1;
+      } else {
+        side(p, threadIdx.x - 32, C::THREADS - 32);
+      }
       __syncthreads();
       if (warp == 0) {
         gj_pivot_block_inverse<LDA>(Acol, pivs[p], fac[p], lane);

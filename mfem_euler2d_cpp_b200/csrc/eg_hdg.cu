@@ -481,14 +481,20 @@ __global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
   for (int e = blockIdx.x; e < g.n; e += gridDim.x) {
     __syncthreads();
     condense_build<Q>(sh, g, fz, u, r, Cb, sf_out, A, nullptr, e, LDA);
-    // [B | r_e] staged in the cell's slot of XY (L2-resident until [X | y]
-    // overwrites it), one element per thread in address order
+    // [B | r_e] is staged in the cell's slot of XY (L2-resident until
+    // [X | y] overwrites it), one element per thread in address order, by
+    // the warps that wait while warp 0 searches each panel's pivots: panel p
+    // stages the p-th of NPAN slices
     double *Rg = XY + (size_t)e * M * NR;
     const double *re = r + (size_t)e * M;
-    for (int i = threadIdx.x; i < M * NR; i += C::THREADS) {
-      const int col = i / M, row = i % M;
-      Rg[i] = col == NR - 1 ? re[row] : lift_entry<Q>(sh.st, sh.SF, row, col);
-    }
+    const auto stage = [&](int p, int t, int nt) {
+      constexpr int SL = (M * NR + NPAN - 1) / NPAN;
+      const int end = min(M * NR, (p + 1) * SL);
+      for (int i = p * SL + t; i < end; i += nt) {
+        const int col = i / M, row = i % M;
+        Rg[i] = col == NR - 1 ? re[row] : lift_entry<Q>(sh.st, sh.SF, row, col);
+      }
+    };
     for (int i = threadIdx.x; i < KR * 32; i += C::THREADS) {
       used[i] = i >= M ? 1 : 0;
       invp[i] = 0;
@@ -496,7 +502,7 @@ __global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
     if (threadIdx.x == 0) sing = 0;
     __syncthreads();
     // ------------------------------------------------ phase 1: reduce A
-    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing);
+    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing, stage);
     // ----------------------------- phase 2: replay on [B | r_e] (registers)
     double acc[TRW][TCW][2];
 #pragma unroll
