@@ -289,14 +289,24 @@ __global__ void __launch_bounds__(32 * WR_ *WC_, MINB)
     }
     if (threadIdx.x == 0) sing = 0;
     __syncthreads();
-    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing);
+    // a panel's 4 columns (with T_r - e_r on its pivot rows) and its T^{-1}
+    // are final once its update is done: the warps waiting while warp 0
+    // searches panel p's pivots write out panel p - 1
+    double *R = rec + (size_t)e * M * M;
+    double *Fo = rec_fac + (size_t)e * NPAN * 16;
+    const auto write_panel = [&](int q, int t, int nt) {
+      for (int i = t; i < 4 * M; i += nt) R[(size_t)q * 4 * M + i] = A[(i % M) + (size_t)(4 * q + i / M) * LDA];
+      for (int i = t; i < 16; i += nt) Fo[q * 16 + i] = fac[q][i];
+    };
+    const auto side = [&](int pp, int t, int nt) {
+      if (pp > 0) write_panel(pp - 1, t, nt);
+    };
+    gj2_reduce<C>(A, topA, rowbuf, fac, pivs, used, invp, &sing, side);
     if (sing) {
       if (threadIdx.x == 0) raise_err(err, DERR_SINGULAR_JACOBI);
       continue;
     }
-    double *R = rec + (size_t)e * M * M;
-    for (int i = threadIdx.x; i < M * M; i += C::THREADS) R[i] = A[(i % M) + (size_t)(i / M) * LDA];
-    for (int i = threadIdx.x; i < NPAN * 16; i += C::THREADS) rec_fac[(size_t)e * NPAN * 16 + i] = fac[i >> 4][i & 15];
+    write_panel(NPAN - 1, threadIdx.x, C::THREADS);
     for (int i = threadIdx.x; i < M; i += C::THREADS) {
       rec_pivs[(size_t)e * M + i] = pivs[i >> 2][i & 3];
       perm[(size_t)e * M + i] = invp[i];
