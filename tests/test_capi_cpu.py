@@ -3,6 +3,7 @@ exports every function include/euler2d_cuda.h declares, builds the
 reference's host tables bit for bit, and the euler2d command line validates
 options exactly like the reference (src/options.cpp) before touching CUDA."""
 import subprocess
+import tempfile
 
 import numpy as np
 import pytest
@@ -57,7 +58,10 @@ def test_host_tables_match_reference(path):
 
 
 def _cli(*args):
-    return subprocess.run([str(CLI), *args], capture_output=True, text=True, timeout=60)
+    # run in a scratch directory: a command line that fails after parsing may
+    # already have created its default output directory (code_test/results)
+    with tempfile.TemporaryDirectory() as tmp:
+        return subprocess.run([str(CLI), *args], capture_output=True, text=True, timeout=60, cwd=tmp)
 
 
 @pytest.mark.parametrize("args,message", [
