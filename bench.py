@@ -51,8 +51,8 @@ WORKLOADS = {
                newton_steps=3,
                label="256x256 periodic Q3 simple wave (gamma=3, alpha=45deg), HDG condensed, FP64"),
 }
-# run to T = 0.2, FP64 and mixed precision, accuracy and
-# conservation of the mixed path against the FP64 path (the FP64 oracle).
+# The 256x256 Q3 accuracy run: to T = 0.2, FP64 and mixed precision, accuracy
+# and conservation of the mixed path against the FP64 path (the FP64 oracle).
 C3_ACCURACY = dict(nx=256, ny=256, k=3, alpha=45.0, form="hdg", precond="block-jacobi", cfl=1.0, end=0.2,
                    label="256x256 periodic Q3 simple wave (gamma=3, alpha=45deg), HDG condensed, SSP-DIRK3 "
                          "CFL 1 to T=0.2, Newton to tol 1e-12, FP64 and mixed precision")
@@ -215,7 +215,7 @@ def run_to_time(w, precision, local):
 
 
 def c3_accuracy(local, cpu: bool):
-    """FP64 and mixed-precision runs to T = 0.2; final L2
+    """256x256 Q3 simple wave: FP64 and mixed-precision runs to T = 0.2; final L2
     errors and conservation drift of both, and the mixed path's error against
     the FP64 path's (the FP64 oracle). cpu: also the reference's CPU cost of
     one Newton update on the same mesh (backward Euler, one update)."""
@@ -259,7 +259,7 @@ def reference_status(nx, k, alpha, steps=3, newton_steps=3, timeout=600.0):
 
 
 def batch_c4(threads: int, cpu: bool):
-    """BASELINE config 4 (64 seeded uneven instances, 3 steps x 3 updates):
+    """The uneven-instance batch (64 seeded instances, nx = ny from 8 to 64, k 1..6, 3 steps x 3 updates):
     the batched mixed-precision path against the plain FP64 path one instance
     at a time; instances that fail here are run through the reference's own
     command line and its outcome is recorded beside them."""
@@ -279,7 +279,7 @@ def batch_c4(threads: int, cpu: bool):
 
 
 def serve_c5():
-    """BASELINE config 5, bounded: 48 requests of its distribution (Poisson
+    """The served request stream, bounded: 48 requests of its distribution (Poisson
     arrivals at 200 requests/s, 1..10 SSP-DIRK3 steps, k 2..6, meshes 20^2 to
     64^2; the full distribution's 128^2 Q7-Q8 requests take minutes each),
     served by 16 workers in mixed precision against the plain FP64 path one
@@ -697,8 +697,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c3", action="store_true", help="skip the 256x256 Q3 run to T=0.2 (FP64 and mixed)")
-    ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch of BASELINE config 4")
-    ap.add_argument("--no-serve", action="store_true", help="skip the 48-request serve sample of BASELINE config 5")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance uneven batch")
+    ap.add_argument("--no-serve", action="store_true", help="skip the 48-request serve sample")
     ap.add_argument("--ref-max-updates", type=int, default=12)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

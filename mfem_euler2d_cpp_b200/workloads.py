@@ -1,7 +1,7 @@
 """Many-instance workloads on one GPU, on the engine's batch and request-loop
 entry points (eg_batch_*, eg_server_*).
 
-batch  Uneven instances run together (BASELINE config 4): `count` seeded
+batch  Uneven instances run together: `count` seeded
        simple-wave problems (gamma = 3) with nx = ny drawn from
        {8,16,24,32,48,64}, k uniform in 1..6 and alpha uniform in (15, 75)
        degrees, each advanced 3 SSP-DIRK3 steps x 3 Newton updates at CFL 1
@@ -38,7 +38,7 @@ import numpy as np
 from . import capi
 
 
-# nx = ny uniform over these sizes, k uniform in 1..6
+# the uneven batch: nx = ny uniform over these sizes, k uniform in 1..6
 C4_SIZES = (8, 16, 24, 32, 48, 64)
 
 
@@ -100,7 +100,7 @@ def run_batch(count=64, seed=0, threads=32, precision="mixed", steps=3, newton_s
         "l2_check": {"instances_checked": checked, "worst_relative_difference_vs_fp64": worst,
                      "all_within_1pct": bool(within)},
         "results_identical_alone_and_batched": bat["errors"] == same_prec["errors"],
-        "config": {"workload": "BASELINE config 4: uneven seeded simple-wave instances", "count": count,
+        "config": {"workload": "uneven seeded simple-wave instances (nx = ny 8..64, k 1..6)", "count": count,
                    "seed": seed, "threads": threads, "precision": precision, "steps": steps,
                    "newton_steps_per_stage": newton_steps, "sizes": list(sizes), "instances": inst},
         "data": "synthetic: seeded simple-wave instances (gamma=3)",
