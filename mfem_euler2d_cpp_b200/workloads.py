@@ -55,6 +55,21 @@ def _joint(errors):
     return float(np.sqrt(np.sum(np.square(errors))))
 
 
+def l2_check(statuses, errors, ref_statuses, ref_errors, bar=0.01):
+    """Every run that completed in both (status 0) has its joint L2 error
+    (the 2-norm of the four component errors) within `bar` (relative) of the
+    reference run's. Returns (checked, worst relative difference, all within)."""
+    checked, worst, within = 0, 0.0, True
+    for st, e, rst, re in zip(statuses, errors, ref_statuses, ref_errors):
+        if st == 0 and rst == 0:
+            e0, e1 = _joint(re), _joint(e)
+            rel = abs(e1 - e0) / e0
+            worst = max(worst, rel)
+            within &= rel <= bar
+            checked += 1
+    return checked, worst, bool(within)
+
+
 def run_batch(count=64, seed=0, threads=32, precision="mixed", steps=3, newton_steps=3, sizes=C4_SIZES):
     """The instances run concurrently in `precision`, against the plain FP64
     path one instance at a time (and `precision` one at a time, which
@@ -79,14 +94,7 @@ def run_batch(count=64, seed=0, threads=32, precision="mixed", steps=3, newton_s
                        "failed": st.failed, "statuses": statuses, "errors": errors}
     bat, ref64 = runs["batched"], runs["fp64_one_at_a_time"]
     same_prec = runs[f"{precision}_one_at_a_time"]
-    checked, worst, within = 0, 0.0, True
-    for i in range(count):
-        if bat["statuses"][i] == 0 and ref64["statuses"][i] == 0:
-            e0, e1 = _joint(ref64["errors"][i]), _joint(bat["errors"][i])
-            rel = abs(e1 - e0) / e0
-            worst = max(worst, rel)
-            within &= rel <= 0.01
-            checked += 1
+    checked, worst, within = l2_check(bat["statuses"], bat["errors"], ref64["statuses"], ref64["errors"])
     return {
         "metric": "accepted Newton updates/s (batched uneven instances)",
         "value": bat["updates_per_s"], "unit": "updates/s", "higher_is_better": True,
@@ -164,14 +172,7 @@ def run_serve(requests=2000, rate=200.0, seed=1, workers=16, budget_gb=120.0, pr
     budget = int(budget_gb * (1 << 30))
     served = _serve(reqs, workers, budget, precision)
     single = _serve(reqs, 1, budget, "fp64")
-    checked, worst, within = 0, 0.0, True
-    for i in range(len(reqs)):
-        if served["statuses"][i] == 0 and single["statuses"][i] == 0:
-            e0, e1 = _joint(single["errors"][i]), _joint(served["errors"][i])
-            rel = abs(e1 - e0) / e0
-            worst = max(worst, rel)
-            within &= rel <= 0.01
-            checked += 1
+    checked, worst, within = l2_check(served["statuses"], served["errors"], single["statuses"], single["errors"])
     for d in (served, single):
         d.pop("errors")
         d["failed_statuses"] = sorted({s for s in d.pop("statuses") if s != 0})

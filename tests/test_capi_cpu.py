@@ -129,3 +129,16 @@ def test_save_solution_rejects_bad_input(tmp_path):
         capi.save_solution(d, np.zeros(7), str(tmp_path / "x"))
     with pytest.raises(capi.EngineError, match="Cannot open solution output"):
         capi.save_solution(d, np.zeros(4 * 9 * 48), str(tmp_path / "missing" / "x"))
+
+
+def test_workload_l2_check_counts_only_runs_that_completed_in_both():
+    """The 1% bar of the batch and serve lines: joint L2 error against the
+    plain FP64 run's, only where both completed."""
+    from mfem_euler2d_cpp_b200 import workloads
+
+    ref = [[3e-7, 4e-7, 0., 0.], [1e-6, 0., 0., 0.], [2e-6, 0., 0., 0.]]
+    ok = [[3e-7, 4e-7, 0., 0.], [1.005e-6, 0., 0., 0.], [9e-6, 0., 0., 0.]]
+    checked, worst, within = workloads.l2_check([0, 0, 20], ok, [0, 0, 0], ref)
+    assert checked == 2 and abs(worst - 0.005) < 1e-12 and within
+    checked, worst, within = workloads.l2_check([0, 0, 0], ok, [0, 0, 0], ref)
+    assert checked == 3 and abs(worst - 3.5) < 1e-12 and not within
