@@ -562,7 +562,9 @@ def run_ours(args, world, rank, local):
     hbm_lines = {}
     for name in ("schur_apply", "recover", "pc_apply", "residual", "dg_apply"):
         ms, cnt = prof[name]
-        per = 2 if name == "schur_apply" else 1
+        # kernels per operation: the Schur action (panel GEMV + face combine) and
+        # the residual (face values, then the cell kernel) launch two
+        per = 2 if name in ("schur_apply", "residual") else 1
         n_op = cnt // per
         if n_op and name in alg:
             avg_s = ms * 1e-3 / n_op

@@ -97,6 +97,10 @@ __global__ void __launch_bounds__(256) admissible_kernel(Geo g, const double *__
 }
 
 // -------------------------------------------- residual / Jacobian action
+// Single-kernel forms, every cell evaluating its own face points (each face
+// point twice). MODE 1 serves the single Jacobian actions; the residual runs
+// as residual_face_kernel + residual_cell_kernel below, with the same
+// arithmetic.
 // MODE 0: r = M^{-1}[-dt sum_q w (Gx F_x + Gy F_y) + lifted HLL fluxes] + u - old
 //         (Problem::Residual, src/problem.cpp:445-507);
 // MODE 1: y = x + M^{-1}[-D_x^T(dt w J_x x) - D_y^T(dt w J_y x) + face lift of
@@ -396,6 +400,112 @@ __global__ void __launch_bounds__(CellCfg<Q>::THREADS)
   }
 }
 
+// Residual face part, once per face point: h = scale (lw F(U_L) + rw F(U_R)
+// + pen (U_L - U_R)) with U_L, U_R the traces on the face's two cells and
+// scale = dt |face| / |K| ew_j (Problem::Residual's numerical flux,
+// src/problem.cpp:470-495; added with + into the left cell, - into the right
+// one). The same arithmetic as the cell-side evaluation it replaces, which
+// computed every face point twice.
+template <int Q>
+__global__ void __launch_bounds__(256) residual_face_kernel(Geo g, const double *__restrict__ tab, Frozen fz,
+                                                            const double *__restrict__ u, double *__restrict__ hface) {
+  __shared__ STab<Q> st;
+  load_tables<Q>(st, tab);
+  __syncthreads();
+  const long long nq = (long long)g.nf * Q;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < nq;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(idx / Q), j = (int)(idx % Q);
+    const int L = f >> 1, axis = f & 1;
+    const int sl = axis ? 3 : 1, sr = sl - 1;
+    const int R = neighbour(L, sl, g.nx, g.ny);
+    double ul[4], ur[4], fl[4], fr[4];
+    trace4<Q>(st, u, L, sl, j, ul);
+    trace4<Q>(st, u, R, sr, j, ur);
+    flux(ul, axis, g.gm1, fl);
+    flux(ur, axis, g.gm1, fr);
+    const double lw = fz.lw[idx], rw = fz.rw[idx], pen = fz.pen[idx];
+    const double len = axis == 0 ? g.hy : g.hx;
+    const double scale = g.dt * len / g.area * st.ew(j);
+    double h[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) h[c] = scale * (lw * fl[c] + rw * fr[c] + pen * (ul[c] - ur[c]));
+    reinterpret_cast<double4 *>(hface)[idx] = make_double4(h[0], h[1], h[2], h[3]);
+  }
+}
+
+// r = M^{-1}[-dt sum_q w (Gx F_x + Gy F_y) + lifted face values] + u - old
+// with the face values of residual_face_kernel (one thread per node,
+// CellCfg<Q>::CPB cells per CTA).
+template <int Q>
+__global__ void __launch_bounds__(CellCfg<Q>::THREADS)
+    residual_cell_kernel(Geo g, const double *__restrict__ tab, const double *__restrict__ u,
+                         const double *__restrict__ old, const double *__restrict__ hface, double *__restrict__ out) {
+  using C = CellCfg<Q>;
+  constexpr int P = C::P, M = C::M, CPB = C::CPB;
+  __shared__ STab<Q> st;
+  __shared__ double fxs[CPB][P][4], fys[CPB][P][4];
+  __shared__ double hs[CPB][4 * Q][4];
+  load_tables<Q>(st, tab);
+  __syncthreads();
+  const int lc = threadIdx.x / P, node = threadIdx.x % P;
+  const int e = blockIdx.x * CPB + lc;
+  const bool active = lc < CPB && e < g.n;
+  double uu[4] = {0., 0., 0., 0.}, oo[4] = {0., 0., 0., 0.};
+  if (active) {
+    const double *v = u + (size_t)e * M + 4 * node;
+    const double *ov = old + (size_t)e * M + 4 * node;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uu[c] = v[c];
+      oo[c] = ov[c];
+    }
+    const double wdt = g.dt * st.w(node);
+    double fx[4], fy[4];
+    flux(uu, 0, g.gm1, fx);
+    flux(uu, 1, g.gm1, fy);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      fxs[lc][node][c] = wdt * fx[c];
+      fys[lc][node][c] = wdt * fy[c];
+    }
+    for (int task = node; task < 4 * Q; task += P) {
+      const int s = task / Q, j = task % Q;
+      const bool own_left = side_is_left(s);
+      const int nb = neighbour(e, s, g.nx, g.ny);
+      const int axis = s < 2 ? 0 : 1;
+      const int f = own_left ? 2 * e + axis : 2 * nb + axis;
+      const double4 h = reinterpret_cast<const double4 *>(hface)[(size_t)f * Q + j];
+      const double sg = own_left ? 1. : -1.;
+      hs[lc][task][0] = sg * h.x;
+      hs[lc][task][1] = sg * h.y;
+      hs[lc][task][2] = sg * h.z;
+      hs[lc][task][3] = sg * h.w;
+    }
+  }
+  __syncthreads();
+  if (!active) return;
+  const int ix = node % Q, iy = node / Q;
+  double acc[4] = {0., 0., 0., 0.};
+#pragma unroll
+  for (int a = 0; a < Q; ++a) {
+    const double dx = st.tdx(a, ix), dy = st.tdy(a, iy);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c] += dx * fxs[lc][iy * Q + a][c] + dy * fys[lc][a * Q + ix][c];
+  }
+  const double w0 = st.fb(0, iy, ix), w1 = st.fb(1, iy, ix);
+  const double w2 = st.fb(2, ix, iy), w3 = st.fb(3, ix, iy);
+  const double im = st.inv_mass(node);
+  double *o = out + (size_t)e * M + 4 * node;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double fc = w0 * hs[lc][0 * Q + iy][c] + w1 * hs[lc][1 * Q + iy][c] + w2 * hs[lc][2 * Q + ix][c] +
+                      w3 * hs[lc][3 * Q + ix][c];
+    const double v = im * (fc - acc[c]);
+    o[c] = v + uu[c] - oo[c];
+  }
+}
+
 template <int Q>
 __host__ __device__ constexpr int lu_rmax() {
   return (4 * Q * Q + 31) / 32;
@@ -607,18 +717,20 @@ void launch_admissible(Ctx &c, const double *u) {
   EG_CUDA(cudaGetLastError());
 }
 
+static int sm_count();
+
 void launch_residual(Ctx &c, const double *u, const double *old, double *r) {
-  ProfScope ps(c, EG_K_RESIDUAL, 1);
+  ProfScope ps(c, EG_K_RESIDUAL, 2);
+  if (!c.dgc_h) c.dgc_h = c.alloc_n<double>((size_t)4 * c.nf * c.q);
+  const int grid = (int)std::min<long long>(((long long)c.nf * c.q + 255) / 256, (long long)sm_count() * 16);
   EG_DISPATCH_Q(c.q, {
     using C = CellCfg<Q>;
     const int blocks = (c.n + C::CPB - 1) / C::CPB;
-    cell_operator_kernel<Q, 0><<<blocks, C::THREADS, 0, c.stream>>>(c.geo, c.tab, frozen_of(c), u,
-                                                                     old, r);
+    residual_face_kernel<Q><<<grid, 256, 0, c.stream>>>(c.geo, c.tab, frozen_of(c), u, c.dgc_h);
+    residual_cell_kernel<Q><<<blocks, C::THREADS, 0, c.stream>>>(c.geo, c.tab, u, old, c.dgc_h, r);
   });
   EG_CUDA(cudaGetLastError());
 }
-
-static int sm_count();
 
 void launch_dg_refresh(Ctx &c, const double *u) {
   ProfScope ps(c, EG_K_DG_APPLY, 1);

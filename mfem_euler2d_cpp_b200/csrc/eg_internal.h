@@ -201,7 +201,7 @@ struct Ctx {
   // DG partial assembly (launch_dg_refresh): dt w J_x, dt w J_y per cell node
   // and lw J(U_L) + pen I, rw J(U_R) - pen I per face point, component-major
   double *dgc_vol = nullptr, *dgc_face = nullptr;
-  double *dgc_h = nullptr;  // the action's face values, 4 per face point
+  double *dgc_h = nullptr;  // face values of the residual and of the cached DG action, 4 per face point
   // --solver dense: the assembled system as a column-major N x N LU with its pivots
   double *dense_a = nullptr;
   int *dense_piv = nullptr;
